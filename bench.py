@@ -1,0 +1,311 @@
+"""Benchmark of the :gradepro estimator on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2|c1|c3]
+
+A "step" is one complete :gradepro estimation (binning, forward transforms, every
+bandwidth step, convergence, outputs) of one sample set.  The default workload is the
+2-D configuration: 1,000,000 samples of a 3-component Gaussian mixture, grid 512 x 512,
+200 bandwidth steps (201 bandwidths), 64 bootstrap resamples -- synthetic, seeded.
+
+value: grid-point.bandwidth-steps per second over all ranks with samples resident in HBM;
+e2e  : the same through the public API (initialize_estimation / estimate_density /
+       get_density) with page-locked host samples copied in and the density copied out
+       every step.
+Multi-GPU: estimations are independent, so each rank runs its own (weak scaling, no
+collective on the data path); timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "parallelkde.jl_b200"))
+sys.path.insert(0, REPO)
+
+import numpy as np  # noqa: E402
+
+METRIC = "KDE estimations/s + grid-pt·steps/s (%HBM peak) vs plain GPU form; p50/p99 ms"
+UNIT = "grid-pt·steps/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def workload(name):
+    from pkde_b200 import workloads as W
+    if name == "c1":
+        x, spec = W.gaussian_1d()
+        return x, dict(dims=spec["dims"], grid_padding=spec["grid_padding"]), dict(n_bootstraps=100, n_steps=None)
+    if name == "c3":
+        x, spec = W.banana_t_3d()
+        return x, dict(dims=spec["dims"]), dict(n_bootstraps=32, n_steps=150)
+    x, spec = W.gmm_2d()
+    return x, dict(dims=spec["dims"]), dict(n_bootstraps=64, n_steps=200)
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(REPO, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+# ----------------------------------------------------------------------- reference arm
+def cpu_reference(x, gspec, kw, budget_s=20.0, log=None):
+    """The oracle port (FP64, scipy.fft threads + OpenMP binning) on a bounded sample:
+    full binning and forward transforms, then bandwidth steps until ~budget_s."""
+    import math
+    import scipy.fft as sfft
+    from oracle import gradepro as og
+    from oracle.rng import bootstrap_indices
+    cores = os.cpu_count() or 1
+    grid = og.find_grid(x, grid_dims=gspec["dims"], grid_padding=gspec.get("grid_padding"))
+    n = x.shape[1]
+    B = kw["n_bootstraps"]
+    idx = bootstrap_indices(1, n, B)
+    t0 = time.perf_counter()
+    Mb, Vb = og.dirac(x, grid, idx, nthreads=cores)
+    Mf, _ = og.dirac(x, grid, np.arange(1, n + 1, dtype=np.int32)[None], include_var=False, nthreads=cores)
+    Mh = og.fourier_statistics(Mb.astype(complex), cores)
+    Vh = og.fourier_statistics(Vb.astype(complex), cores)
+    Fh = og.fourier_statistics(Mf.astype(complex), cores)[0]
+    t_setup = time.perf_counter() - t0
+    times, sl, so, eps = og.ladder(x, grid, kw["n_steps"])
+    S = len(times)
+    tinit = og.initial_bandwidth(grid)
+    done = 0
+    t1 = time.perf_counter()
+    with np.errstate(all="ignore"):
+        while done < S and (time.perf_counter() - t1) < budget_s:
+            t = times[done]
+            Mt, Vt = og.propagate_statistics(Mh, Vh, grid, t, tinit)
+            og.scaled_vmr(og.ifourier_statistics(Mt, True, cores), og.ifourier_statistics(Vt, True, cores), t, tinit, n)
+            og.full_means(og.ifourier_statistics(og.propagate_means(Fh, grid, t), False, cores))
+            done += 1
+    t_steps = time.perf_counter() - t1
+    G = grid.size
+    per_step = t_steps / done
+    t_full = t_setup + per_step * S
+    value = G * S / t_full
+    sample = (f"oracle FP64 port, {cores} threads: binning + forward FFTs of all {B} resamples ({t_setup:.1f} s) "
+              f"and {done} of {S} bandwidth steps ({t_steps:.1f} s); full-estimation time extrapolated "
+              f"as setup + {S} x per-step = {t_full:.1f} s")
+    return dict(value=value, unit=UNIT, cores=cores, kind="port", sample=sample, est_per_s=1.0 / t_full)
+
+
+# ---------------------------------------------------------------------------- our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local, dist = dist_setup(args)
+    x, gspec, kw = workload(args.workload)
+    wl_name = {"c1": "1-D N(0,1) n=1e4, 1024 pts, B=100, 251 bandwidths",
+               "c2": "2-D 3-GMM n=1e6, 512x512, B=64, 201 bandwidths",
+               "c3": "3-D banana+t3 n=4e6, 128^3, B=32, 151 bandwidths"}[args.workload]
+
+    if args.impl == "reference":
+        if rank == 0:
+            ref = cpu_reference(x, gspec, kw, budget_s=args.cpu_budget)
+            line = {"impl": "reference", "metric": METRIC, "value": ref["value"], "unit": UNIT, "n_gpus": args.gpus,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / ref["est_per_s"],
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic", "config": {"workload": wl_name, "estimations_per_s": ref["est_per_s"]},
+                    "cpu_baseline": {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                    "e2e": {"value": ref["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import pkde_b200 as pk
+    from pkde_b200 import _lib, raw
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pk.load()
+    pk.context(local)
+    grid = pk.find_grid(x, grid_dims=gspec["dims"], grid_padding=gspec.get("grid_padding"))
+    G = int(np.prod(grid.dims))
+    n, N = x.shape[1], x.shape[0]
+    S = (kw["n_steps"] or 250) + 1
+    samples = torch.from_numpy(np.ascontiguousarray(x.T)).to(dev)
+    dens = torch.empty(G, dtype=torch.float64, device=dev)
+    sel = torch.empty(G, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def one(seed):
+        raw.gradepro_device(grid, samples, n, dens, sel, seed=seed, stream=sp, device_id=local,
+                            n_bootstraps=kw["n_bootstraps"], n_steps=kw["n_steps"])
+
+    for w in range(args.warmup):
+        one(1000 + w)
+    # timed region: K estimations, samples resident in HBM; profiling events on
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    _lib.get_stats(local, reset=True)
+    _lib.set_profiling(True, local)
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lat = []
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for k in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        one(rank * 100000 + k)
+        b.record(stream)
+        lat.append((a, b))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    _lib.set_profiling(False, local)
+    stats = _lib.get_stats(local, reset=True)
+    elapsed_ms = ev0.elapsed_time(ev1)
+    lat_ms = sorted(a.elapsed_time(b) for a, b in lat)
+    t_max = elapsed_ms
+    if dist:
+        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    units = G * S * args.steps * world
+    value = units / (t_max / 1000.0)
+
+    # e2e through the public API with page-locked host samples
+    est = pk.initialize_estimation(x, grid=grid)
+    est.kde.pin()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = time.perf_counter()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for k in range(args.steps):
+        pk.estimate_density(est, "gradepro", n_bootstraps=kw["n_bootstraps"], n_steps=kw["n_steps"],
+                            seed=rank * 100000 + k, device_id=local)
+        pk.get_density(est)
+    ev3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max(ev2.elapsed_time(ev3), (time.perf_counter() - e0) * 1000.0)
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = units / (e2e_ms / 1000.0)
+
+    # roofline of the per-bandwidth-step pipeline: FP64 spectra (2 bootstraps' means or
+    # second moments per complex array, plus the full-sample means) read once per step:
+    # 16 (B + 1) bytes per grid point per step.
+    B = kw["n_bootstraps"]
+    peak, peak_kind = peaks()
+    step_phases = ["step_fft", "step_vmr", "step_means"]
+    step_ms = sum(stats["phase_ms"][p] for p in step_phases) / args.steps
+    step_launches = sum(stats["phase_launches"][p] for p in step_phases) / args.steps
+    alg_bytes = 16.0 * (B + 1) * G * S
+    achieved = alg_bytes / (step_ms / 1000.0) / 1e9 if step_ms > 0 else None
+    dominant = max(stats["phase_ms"], key=lambda p: stats["phase_ms"][p])
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl_name, "grid_points": G, "bandwidths": S, "bootstraps": B, "samples": n,
+                   "estimations_per_s": args.steps * world / (t_max / 1000.0),
+                   "p50_ms": lat_ms[len(lat_ms) // 2], "p99_ms": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))],
+                   "l2": "inputs (spectra 16(B+1)G bytes) larger than the 126 MB L2",
+                   "parallelism": f"independent estimations per rank x{world}"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n * N * 8),
+                "d2h_bytes_per_step": int(G * 12)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "kernel": "per-bandwidth-step pipeline (step_fft + step_vmr + step_means)",
+                     "peak_source": peak_kind, "step_ms_per_estimation": step_ms,
+                     "launches_per_estimation": step_launches},
+        "phase_ms_per_estimation": {p: v / args.steps for p, v in stats["phase_ms"].items()},
+        "dominant_phase": dominant,
+        "gpu_launches": stats["launches"],
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        ref = cpu_reference(x, gspec, kw, budget_s=args.cpu_budget)
+        line["cpu_baseline"] = {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+/*
+ * pkde_b200 -- C ABI of the B200 (sm_100a) implementation of ParallelKDE.jl's
+ * `:gradepro` grid estimator (the `device=:cuda` path).
+ *
+ * Plain C types only; no CUDA or torch types appear in the signatures.  A `stream`
+ * argument is a `cudaStream_t` passed as `void*` (NULL = the legacy default stream).
+ *
+ * Layout conventions (those of the reference, ParallelKDE.jl):
+ *   - samples: N x n, column-major (the N coordinates of one sample are contiguous);
+ *   - grid arrays: column-major, grid axis 1 fastest; G = prod(dims);
+ *   - bootstrap indices: n x B, column-major, 1-based (like `rand(1:n, n, B)`).
+ *
+ * Error handling: every entry point returns a pkde_status; on failure the message is
+ * available from pkde_last_error(ctx).  PKDE_EINVAL corresponds to the reference's
+ * ArgumentError.  Calls on one context are not reentrant (one host thread at a time).
+ */
+#ifndef PKDE_B200_H
+#define PKDE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pkde_status {
+  PKDE_OK = 0,
+  PKDE_EINVAL = 1,      /* invalid argument; data beyond the grid (ArgumentError) */
+  PKDE_ENOMEM = 2,      /* device allocation failed */
+  PKDE_ECUDA = 3,       /* CUDA runtime error */
+  PKDE_EUNSUPPORTED = 4 /* valid request this build does not handle */
+} pkde_status;
+
+/* flags for the pointer arguments */
+#define PKDE_DEVICE_INPUT 1u  /* data / indices / input arrays are device pointers */
+#define PKDE_DEVICE_OUTPUT 2u /* output arrays are device pointers */
+
+typedef struct pkde_ctx pkde_ctx;
+
+/* Uniform grid, one entry per axis (axis 1 first).  Mirrors Grid/CuGrid
+ * (src/Grids/Grids.jl:67-134): lo/hi are the extrema of the coordinate range
+ * (low_bounds/high_bounds, :203-210), h the step (spacings, :189). */
+typedef struct pkde_grid {
+  int32_t ndim; /* 1..4 */
+  int32_t reserved;
+  int64_t dims[4];
+  double lo[4];
+  double hi[4];
+  double h[4];
+} pkde_grid;
+
+/* Keyword arguments of estimate_density!(est, :gradepro; ...)
+ * (docs/src/estimators/gradepro.md:19-28, src/DensityEstimators/GradeProEstimator.jl:700-858).
+ * NaN selects the reference default. */
+typedef struct pkde_gradepro_params {
+  pkde_grid grid;
+  int32_t n_bootstraps; /* B >= 2 (default 100, GradeProEstimator.jl:705) */
+  int32_t n_steps;      /* > 0: S = n_steps + 1 bandwidths; 0: use bw_step, else 250 */
+  double bw_step;       /* bandwidth step (all axes); NaN: unused */
+  double bw_final[4];   /* final bandwidth per axis; NaN: Silverman's rule */
+  double alpha_s;       /* NaN: 0.0 for 1-D, 0.06 otherwise */
+  double alpha_os;      /* NaN: 0.1 */
+  double eps;           /* NaN: 2.0 for 1-D, -0.5 otherwise */
+} pkde_gradepro_params;
+
+/* Context: owns the device state and scratch of one GPU.
+ * Replaces the device set-up of initialize_estimation (src/ParallelKDE.jl:102-158). */
+int pkde_create(pkde_ctx **ctx, int device);
+int pkde_destroy(pkde_ctx *ctx);
+const char *pkde_last_error(const pkde_ctx *ctx);
+const char *pkde_version(void);
+
+/* Fill `p` with the reference defaults for an `ndim`-dimensional grid (grid left zeroed). */
+int pkde_gradepro_default_params(pkde_gradepro_params *p, int32_t ndim);
+
+/* The hot path: estimate_density!(est, :gradepro; kwargs...) for one sample set.
+ * Replaces src/DensityEstimators/DensityEstimators.jl:58-84 (estimate!(::Symbol, kde))
+ * -> GradeProEstimator.jl:700-858 (initialize_estimator) -> :968-1051 (estimate!)
+ * -> :1053-1072 (replace_nans!) on the CUDA device.
+ *   data        : N x n samples (FP64)
+ *   boot_idx    : n x B 1-based bootstrap draws, or NULL to draw them from `seed`
+ *                 with the counter-based generator documented in pkde_boot_index
+ *   density_out : G densities (FP64, column-major grid order)
+ *   selected_out: G int32, the 0-based bandwidth step whose means were kept per grid
+ *                 point, or S when replace_nans! filled the point (may be NULL)
+ * Samples on or beyond the grid bounds give PKDE_EINVAL with the reference's message
+ * (DirectSpace.jl:479-512). */
+int pkde_gradepro_estimate(pkde_ctx *ctx, const pkde_gradepro_params *p, const double *data,
+                           int64_t n, const int32_t *boot_idx, uint64_t seed, double *density_out,
+                           int32_t *selected_out, uint32_t flags, void *stream);
+
+/* Dirac-sequence binning of bootstrap resamples onto the grid.
+ * Replaces initialize_dirac_sequence(Val(:cuda), ...) (DirectSpace.jl:289-362) and its
+ * kernel generate_dirac_cuda! (:364-477), following the CPU arithmetic (:196-287).
+ *   means_out : G x B FP64 (sum of corner weights per cell)       (may be NULL)
+ *   sq_out    : G x B FP64 (sum of squared corner weights)        (may be NULL)
+ *   counts_out: G x B uint32, draws whose lower cell is the cell  (may be NULL)
+ * boot_idx NULL with nboot == 0 bins the identity resample (all samples once). */
+int pkde_dirac_sequence(pkde_ctx *ctx, const pkde_grid *grid, const double *data, int64_t n,
+                        const int32_t *boot_idx, int32_t nboot, uint64_t seed, double *means_out,
+                        double *sq_out, uint32_t *counts_out, uint32_t flags, void *stream);
+
+/* N-D complex FFT of `batch` arrays of G complex values (interleaved re, im FP64).
+ * direction -1: forward, unnormalised (fourier_statistics!, FourierSpace.jl:25-104);
+ * direction +1: inverse scaled by 1/G (ifourier_statistics!, FourierSpace.jl:445-524). */
+int pkde_fft(pkde_ctx *ctx, int32_t ndim, const int64_t *dims, double *data, int32_t batch,
+             int32_t direction, uint32_t flags, void *stream);
+
+/* Scaled variance-to-mean ratio of B bootstrap means/second-moment arrays
+ * (complex, G x B): calculate_scaled_vmr! (DirectSpace.jl:526-740).
+ * vmr_out: G values log(prod(t^2+t0^2)^(3/2) n^3 var_b(vmr)) or NaN. */
+int pkde_scaled_vmr(pkde_ctx *ctx, int64_t G, int32_t nboot, const double *means,
+                    const double *sq, int32_t ndim, const double *t, const double *t0,
+                    int64_t n_samples, double *vmr_out, uint32_t flags, void *stream);
+
+/* One convergence update per grid point: identify_convergence! / find_stability
+ * (DirectSpace.jl:829-1100).  All arrays have G entries and are updated in place;
+ * `flags` bit PKDE_DEVICE_INPUT says they are device pointers. */
+int pkde_identify_convergence(pkde_ctx *ctx, int64_t G, double *density, const double *means,
+                              const double *vmr_current, const double *vmr_prev1,
+                              const double *vmr_prev2, double dlogt, double eps, int64_t steps_low,
+                              int64_t steps_over, double *minima, uint16_t *counters_low,
+                              uint16_t *counters_over, uint8_t *low_density_flags, uint32_t flags,
+                              void *stream);
+
+/* Launch accounting and per-phase device time, for tracing and the roofline report.
+ * No counterpart in the reference, which has no tracing.
+ * When enabled, every kernel the context launches is bracketed by CUDA events on its
+ * stream and its elapsed time is added to its phase when the call synchronises. */
+#define PKDE_NPHASES 6
+typedef enum pkde_phase {
+  PKDE_PHASE_BINNING = 0,      /* binning + fixed-point conversion */
+  PKDE_PHASE_FORWARD_FFT = 1,  /* forward transforms, once per estimation */
+  PKDE_PHASE_STEP_FFT = 2,     /* per-bandwidth-step inverse FFT passes (axes N..2) */
+  PKDE_PHASE_STEP_VMR = 3,     /* per-step fused axis-1 inverse FFT + VMR + bootstrap variance */
+  PKDE_PHASE_STEP_MEANS = 4,   /* per-step means + convergence update */
+  PKDE_PHASE_OTHER = 5         /* moments, state init, replace_nans */
+} pkde_phase;
+
+typedef struct pkde_stats {
+  uint64_t launches;                  /* kernels launched since the last reset */
+  uint64_t phase_launches[PKDE_NPHASES];
+  double phase_ms[PKDE_NPHASES];      /* device time per phase (profiling enabled only) */
+} pkde_stats;
+
+int pkde_set_profiling(pkde_ctx *ctx, int enable);
+int pkde_get_stats(pkde_ctx *ctx, pkde_stats *out, int reset);
+
+/* Counter-based bootstrap draw used when boot_idx is NULL (0-based result):
+ *   x = seed + (b*n + j + 1) * 0x9E3779B97F4A7C15 (mod 2^64), z = splitmix64(x),
+ *   idx = ((z >> 32) * n) >> 32.
+ * No counterpart in the reference, whose Julia RNG streams are not reproducible
+ * outside Julia (src/KDEs/KDEs.jl:182-206). */
+int64_t pkde_boot_index(uint64_t seed, int64_t n, int64_t b, int64_t j);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PKDE_B200_H */

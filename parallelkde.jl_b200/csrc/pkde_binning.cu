@@ -1,0 +1,378 @@
+// Dirac-sequence binning (cloud-in-cell of every bootstrap resample onto the grid).
+//
+// Reference: src/StatisticsPropagation/DirectSpace.jl:196-242 (generate_dirac_cpu!, the
+// FP64 arithmetic followed here), :364-477 (generate_dirac_cuda!, FP32 atomics),
+// :479-512 (check_data).
+//
+// B200 design: the per-sample arithmetic (cell index, remainders, the 2^N corner terms)
+// is done once per sample in FP64 exactly as the reference's CPU path does it; each
+// term is then quantised to a 64-bit fixed-point integer with a power-of-two scale
+// chosen from the exact per-cell draw counts, so that the per-cell sums are exact
+// integer sums: independent of the order in which the atomics land, and within one
+// rounding of the term values.  Draws are processed bootstrap-major so the atomics of
+// one bootstrap column stay in L2.
+#include <cstring>
+
+#include "pkde_internal.cuh"
+
+namespace pkde {
+namespace {
+
+constexpr int kThreads = 256;
+
+struct GridDev {
+  int ndim;
+  int64_t dims[4];
+  int64_t stride[4];
+  double lo[4], hi[4], h[4];
+};
+
+GridDev to_dev(const pkde_grid *g) {
+  GridDev d{};
+  d.ndim = g->ndim;
+  int64_t s = 1;
+  for (int j = 0; j < g->ndim; ++j) {
+    d.dims[j] = g->dims[j];
+    d.stride[j] = s;
+    s *= g->dims[j];
+    d.lo[j] = g->lo[j];
+    d.hi[j] = g->hi[j];
+    d.h[j] = g->h[j];
+  }
+  return d;
+}
+
+// Per sample: bounds check, lower cell, remainders r_h (DirectSpace.jl:219-224).
+__global__ void prepass_kernel(GridDev g, const double *__restrict__ data, int64_t n,
+                               uint32_t *__restrict__ cell, double *__restrict__ rh, int *err) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  int64_t c = 0;
+  bool bad_bound = false, bad_top = false;
+  for (int j = 0; j < g.ndim; ++j) {
+    double x = data[s * g.ndim + j];
+    if ((x >= g.hi[j]) | (x <= g.lo[j]) | !(x == x)) bad_bound = true;
+    double delta = __dsub_rn(x, g.lo[j]);
+    double l = floor(__ddiv_rn(delta, g.h[j]));
+    double r = fmod(delta, g.h[j]);
+    if (!bad_bound && (l + 1.0 >= (double)g.dims[j] || l < 0.0)) bad_top = true;
+    int64_t li = bad_bound || bad_top ? 0 : (int64_t)l;
+    c += li * g.stride[j];
+    rh[j * n + s] = r;
+  }
+  if (bad_bound) atomicOr(err, 1);
+  if (bad_top) atomicOr(err, 2);
+  cell[s] = (uint32_t)c;
+}
+
+__device__ __forceinline__ int64_t draw_sample(int64_t b, int64_t j, int64_t n, int64_t nboot,
+                                               const int32_t *__restrict__ idx, uint64_t seed, int *err) {
+  if (b == nboot) return j;  // identity resample (B = 0 in the reference)
+  if (idx) {
+    int64_t v = (int64_t)idx[b * n + j] - 1;
+    if (v < 0 || v >= n) {
+      atomicOr(err, 4);
+      return 0;
+    }
+    return v;
+  }
+  return boot_draw(seed, n, b, j);
+}
+
+// counts[b][cell]: draws of resample b whose lower cell is `cell` (slot nboot = identity).
+__global__ void count_kernel(const uint32_t *__restrict__ cell, int64_t n, int64_t nslots, int64_t nboot,
+                             int64_t G, const int32_t *__restrict__ idx, uint64_t seed,
+                             uint32_t *__restrict__ counts, int *err) {
+  const int64_t total = nslots * n;
+  for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < total;
+       d += (int64_t)gridDim.x * blockDim.x) {
+    int64_t b = d / n;
+    int64_t j = d - b * n;
+    int64_t slot_b = b < nboot ? b : nboot;  // slots beyond nboot only exist for identity
+    int64_t s = draw_sample(slot_b, j, n, nboot, idx, seed, err);
+    atomicAdd(&counts[b * G + cell[s]], 1u);
+  }
+}
+
+__global__ void max_kernel(const uint32_t *__restrict__ v, int64_t m, unsigned int *out) {
+  uint32_t best = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x)
+    best = max(best, v[i]);
+  for (int o = 16; o > 0; o >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, best);
+}
+
+// Per sample: the 2^N corner terms of DirectSpace.jl:227-237, quantised.
+// Corner c: axis j (0-based) takes the lower cell iff bit (N-1-j) of c is set.
+__global__ void quantize_kernel(GridDev g, const double *__restrict__ rh, int64_t n, double denom,
+                                int e_m, int e_v, unsigned long long *__restrict__ qm,
+                                unsigned long long *__restrict__ qv) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int N = g.ndim;
+  double r_h[4], r_l[4];
+  for (int j = 0; j < N; ++j) {
+    r_h[j] = rh[j * n + s];
+    r_l[j] = __dsub_rn(g.h[j], r_h[j]);
+  }
+  const int nc = 1 << N;
+  for (int c = 0; c < nc; ++c) {
+    double pl = 1.0, ph = 1.0;
+    bool fl = false, fh = false;
+    for (int j = 0; j < N; ++j) {
+      if ((c >> (N - 1 - j)) & 1) {
+        pl = fl ? __dmul_rn(pl, r_l[j]) : r_l[j];
+        fl = true;
+      } else {
+        ph = fh ? __dmul_rn(ph, r_h[j]) : r_h[j];
+        fh = true;
+      }
+    }
+    double term = __ddiv_rn(__dmul_rn(pl, ph), denom);
+    double sq = __dmul_rn(term, term);
+    qm[c * n + s] = __double2ull_rn(ldexp(term, e_m));
+    if (qv) qv[c * n + s] = __double2ull_rn(ldexp(sq, e_v));
+  }
+}
+
+// Scatter of the quantised terms.  Destination u64 slot of (resample b, cell, array):
+//   paired layout (spectra): ((2*(b/2) + arr) * G + cell) * 2 + (b % 2), identity slot
+//   (b == nboot) at (2*npairs*G + cell) * 2;  plain layout: arr_base[arr] + b*G + cell.
+template <bool PAIRED>
+__global__ void weight_kernel(const uint32_t *__restrict__ cell, int64_t n, int64_t nslots, int64_t nboot,
+                              int64_t G, int ndim, const int64_t *__restrict__ corner_off,
+                              const int32_t *__restrict__ idx, uint64_t seed,
+                              const unsigned long long *__restrict__ qm,
+                              const unsigned long long *__restrict__ qv, unsigned long long *__restrict__ outM,
+                              unsigned long long *__restrict__ outV, int64_t npairs, int *err) {
+  const int64_t total = nslots * n;
+  const int nc = 1 << ndim;
+  for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < total;
+       d += (int64_t)gridDim.x * blockDim.x) {
+    int64_t b = d / n;
+    int64_t j = d - b * n;
+    int64_t s = draw_sample(b < nboot ? b : nboot, j, n, nboot, idx, seed, err);
+    int64_t c0 = cell[s];
+    for (int c = 0; c < nc; ++c) {
+      int64_t cc = c0 + corner_off[c];
+      unsigned long long m = qm[c * n + s];
+      if (PAIRED) {
+        if (b == nboot) {
+          atomicAdd(&outM[(2 * npairs * G + cc) * 2], m);
+        } else {
+          int64_t p = b >> 1, lane = b & 1;
+          atomicAdd(&outM[((2 * p) * G + cc) * 2 + lane], m);
+          if (qv) atomicAdd(&outM[((2 * p + 1) * G + cc) * 2 + lane], qv[c * n + s]);
+        }
+      } else {
+        atomicAdd(&outM[b * G + cc], m);
+        if (qv && outV && b < nboot) atomicAdd(&outV[b * G + cc], qv[c * n + s]);
+      }
+    }
+  }
+}
+
+// In-place conversion of the fixed-point sums to FP64 (same 8-byte slots).
+__global__ void dequant_kernel(unsigned long long *v, int64_t m, double scale) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    unsigned long long x = v[i];
+    reinterpret_cast<double *>(v)[i] = (double)x * scale;
+  }
+}
+
+__global__ void dequant_paired_kernel(unsigned long long *v, int64_t G, int64_t npairs, double sm, double sv) {
+  // arrays: [z0, w0, z1, w1, ..., zF]; w arrays use sv
+  const int64_t total = (2 * npairs + 1) * G * 2;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t arr = i / (2 * G);
+    double sc = (arr < 2 * npairs && (arr & 1)) ? sv : sm;
+    unsigned long long x = v[i];
+    reinterpret_cast<double *>(v)[i] = (double)x * sc;
+  }
+}
+
+int grid_blocks(pkde_ctx *ctx, int64_t work) {
+  int64_t b = (work + kThreads - 1) / kThreads;
+  int64_t cap = (int64_t)ctx->sm_count * 16;
+  return (int)std::max<int64_t>(1, std::min(b, cap));
+}
+
+}  // namespace
+
+// Shared driver.  d_data, d_idx are device pointers.  If `paired_out` is given, the
+// bootstrap means/squares are written as the paired complex layout used by the
+// estimator (z_p = M_2p + i M_2p+1, w_p = V_2p + i V_2p+1, zF = M_identity + 0i);
+// otherwise plain G x nboot FP64 arrays (and/or the identity when nboot == 0).
+struct DiracScales {
+  double sm, sv;
+};
+
+static DiracScales dirac_core(pkde_ctx *ctx, const pkde_grid *g, const double *d_data, int64_t n,
+                              const int32_t *d_idx, int64_t nboot, bool with_identity, uint64_t seed,
+                              bool want_sq, double2 *paired_out, double *plain_m, double *plain_v,
+                              uint32_t *d_counts_out, cudaStream_t st) {
+  grid_validate(g);
+  if (n < 1 || n >= (int64_t(1) << 31)) throw invalid("number of samples must be in [1, 2^31)");
+  GridDev gd = to_dev(g);
+  const int64_t G = grid_size(g);
+  const int N = g->ndim;
+  const int nc = 1 << N;
+  const int64_t nslots = nboot + (with_identity ? 1 : 0);
+
+  // scratch: cell (u32 n), rh (N*n f64), counts (nslots*G u32), q arrays (nc*n u64 x2), misc
+  uint32_t *cell = (uint32_t *)ensure(ctx, BUF_PRE_CELL, sizeof(uint32_t) * n);
+  double *rh = (double *)ensure(ctx, BUF_PRE_RH, sizeof(double) * N * n + sizeof(unsigned long long) * 2 * nc * n);
+  unsigned long long *qm = reinterpret_cast<unsigned long long *>(rh + N * n);
+  unsigned long long *qv = qm + (int64_t)nc * n;
+  uint32_t *counts = (uint32_t *)ensure(ctx, BUF_COUNTS, sizeof(uint32_t) * nslots * G);
+  int *misc = (int *)ensure(ctx, BUF_MISC, 256);
+  int *err = misc;
+  unsigned int *maxc = reinterpret_cast<unsigned int *>(misc + 1);
+  int64_t *corner_off = reinterpret_cast<int64_t *>(misc + 8);  // 16 entries
+
+  int64_t off_h[16];
+  for (int c = 0; c < nc; ++c) {
+    int64_t o = 0;
+    for (int j = 0; j < N; ++j)
+      if (!((c >> (N - 1 - j)) & 1)) o += gd.stride[j];
+    off_h[c] = o;
+  }
+  PKDE_CUDA_TRY(cudaMemsetAsync(misc, 0, 64, st));
+  PKDE_CUDA_TRY(cudaMemcpyAsync(corner_off, off_h, sizeof(int64_t) * nc, cudaMemcpyHostToDevice, st));
+  PKDE_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nslots * G, st));
+
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    prepass_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(gd, d_data, n, cell, rh, err);
+  }
+  PKDE_CHECK_LAUNCH();
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    count_kernel<<<grid_blocks(ctx, nslots * n), kThreads, 0, st>>>(cell, n, nslots, nboot, G, d_idx, seed, counts, err);
+  }
+  PKDE_CHECK_LAUNCH();
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    max_kernel<<<grid_blocks(ctx, nslots * G), kThreads, 0, st>>>(counts, nslots * G, maxc);
+  }
+  PKDE_CHECK_LAUNCH();
+  int hbuf[2];
+  PKDE_CUDA_TRY(cudaMemcpyAsync(hbuf, misc, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+  PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+  if (hbuf[0] & 1) throw invalid("Data points lie beyond grid. Remove them or increase grid boundaries.");
+  if (hbuf[0] & 2)
+    throw invalid("Data points lie within one rounding of the upper grid bound. Remove them or increase grid boundaries.");
+  if (hbuf[0] & 4) throw invalid("Bootstrap indices must lie in 1:n_samples.");
+  const double cmax = (double)(uint32_t)hbuf[1];
+
+  // term <= prod(h) / (n prod(h)^2); a cell sums at most 2^N * cmax terms.
+  double sp = g->h[0];
+  for (int j = 1; j < N; ++j) sp = sp * g->h[j];
+  const double denom = (double)n * (sp * sp);
+  const double tmax = (1.0 / ((double)n * sp)) * (1.0 + 1e-12);
+  const double bound_m = (double)nc * std::max(cmax, 1.0) * tmax;
+  const double bound_v = (double)nc * std::max(cmax, 1.0) * tmax * tmax;
+  int ex_m, ex_v;
+  std::frexp(bound_m, &ex_m);  // bound_m < 2^ex_m
+  std::frexp(bound_v, &ex_v);
+  const int e_m = 62 - ex_m;
+  const int e_v = 62 - ex_v;
+
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    quantize_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(gd, rh, n, denom, e_m, e_v, qm,
+                                                                                     want_sq ? qv : nullptr);
+  }
+  PKDE_CHECK_LAUNCH();
+  const double sm = std::ldexp(1.0, -e_m), sv = std::ldexp(1.0, -e_v);
+  if (paired_out) {
+    const int64_t npairs = (nboot + 1) / 2;
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(paired_out);
+    PKDE_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double2) * (2 * npairs + 1) * G, st));
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+      weight_kernel<true><<<grid_blocks(ctx, nslots * n), kThreads, 0, st>>>(
+          cell, n, nslots, nboot, G, N, corner_off, d_idx, seed, qm, want_sq ? qv : nullptr, acc, nullptr, npairs, err);
+    }
+    PKDE_CHECK_LAUNCH();
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+      dequant_paired_kernel<<<grid_blocks(ctx, (2 * npairs + 1) * G * 2), kThreads, 0, st>>>(acc, G, npairs, sm, sv);
+    }
+    PKDE_CHECK_LAUNCH();
+  } else {
+    unsigned long long *am = reinterpret_cast<unsigned long long *>(plain_m);
+    unsigned long long *av = reinterpret_cast<unsigned long long *>(plain_v);
+    PKDE_CUDA_TRY(cudaMemsetAsync(am, 0, sizeof(double) * nslots * G, st));
+    if (av) PKDE_CUDA_TRY(cudaMemsetAsync(av, 0, sizeof(double) * nboot * G, st));
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+      weight_kernel<false><<<grid_blocks(ctx, nslots * n), kThreads, 0, st>>>(
+          cell, n, nslots, nboot, G, N, corner_off, d_idx, seed, qm, (want_sq && av) ? qv : nullptr, am, av, 0, err);
+    }
+    PKDE_CHECK_LAUNCH();
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+      dequant_kernel<<<grid_blocks(ctx, nslots * G), kThreads, 0, st>>>(am, nslots * G, sm);
+    }
+    PKDE_CHECK_LAUNCH();
+    if (av) {
+      {
+        ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+        dequant_kernel<<<grid_blocks(ctx, nboot * G), kThreads, 0, st>>>(av, nboot * G, sv);
+      }
+      PKDE_CHECK_LAUNCH();
+    }
+  }
+  if (d_counts_out) PKDE_CUDA_TRY(cudaMemcpyAsync(d_counts_out, counts, sizeof(uint32_t) * nslots * G,
+                                                  cudaMemcpyDeviceToDevice, st));
+  return DiracScales{sm, sv};
+}
+
+// Estimator entry: paired spectra-ready layout (nboot resamples + identity).
+void dirac_paired(pkde_ctx *ctx, const pkde_grid *g, const double *d_data, int64_t n, const int32_t *d_idx,
+                  int64_t nboot, uint64_t seed, double2 *spectra, cudaStream_t st) {
+  dirac_core(ctx, g, d_data, n, d_idx, nboot, true, seed, true, spectra, nullptr, nullptr, nullptr, st);
+}
+
+}  // namespace pkde
+
+extern "C" int pkde_dirac_sequence(pkde_ctx *ctx, const pkde_grid *grid, const double *data, int64_t n,
+                                   const int32_t *boot_idx, int32_t nboot, uint64_t seed, double *means_out,
+                                   double *sq_out, uint32_t *counts_out, uint32_t flags, void *stream) {
+  return pkde_guard(ctx, [&] {
+    using namespace pkde;
+    if (!ctx) throw invalid("context is NULL");
+    PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    grid_validate(grid);
+    if (nboot < 0) throw invalid("Number of bootstraps must be non-negative");
+    if (!data) throw invalid("data is NULL");
+    const bool din = flags & PKDE_DEVICE_INPUT, dout = flags & PKDE_DEVICE_OUTPUT;
+    const int N = grid->ndim;
+    const int64_t G = grid_size(grid);
+    const bool identity = nboot == 0;
+    const int64_t nb = identity ? 0 : nboot;
+    const int64_t nslots = identity ? 1 : nb;
+    double *d_data = (double *)ensure(ctx, BUF_DATA, sizeof(double) * N * n);
+    copy_in(d_data, data, sizeof(double) * N * n, din, st);
+    int32_t *d_idx = nullptr;
+    if (!identity && boot_idx) {
+      d_idx = (int32_t *)ensure(ctx, BUF_IDX, sizeof(int32_t) * n * nb);
+      copy_in(d_idx, boot_idx, sizeof(int32_t) * n * nb, din, st);
+    }
+    double *om = (double *)ensure(ctx, BUF_OUT, sizeof(double) * (2 * nslots * G) + sizeof(uint32_t) * nslots * G);
+    double *ov = om + nslots * G;
+    uint32_t *oc = reinterpret_cast<uint32_t *>(ov + nslots * G);
+    dirac_core(ctx, grid, d_data, n, d_idx, nb, identity, seed, sq_out != nullptr && !identity, nullptr, om,
+               (sq_out && !identity) ? ov : nullptr, oc, st);
+    if (means_out) copy_out(means_out, om, sizeof(double) * nslots * G, dout, st);
+    if (sq_out && !identity) copy_out(sq_out, ov, sizeof(double) * nslots * G, dout, st);
+    if (sq_out && identity) {
+      if (dout) PKDE_CUDA_TRY(cudaMemsetAsync(sq_out, 0, sizeof(double) * G, st));
+      else std::memset(sq_out, 0, sizeof(double) * G);
+    }
+    if (counts_out) copy_out(counts_out, oc, sizeof(uint32_t) * nslots * G, dout, st);
+    PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+  });
+}

@@ -1,0 +1,464 @@
+// Internal definitions shared by the pkde_b200 CUDA sources: context, status handling,
+// device buffers, FP64 complex helpers and the shared-memory mixed-radix FFT.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/pkde_b200.h"
+
+namespace pkde {
+
+// ----------------------------------------------------------------------------- status
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define PKDE_CUDA_TRY(expr)                                                                     \
+  do {                                                                                          \
+    cudaError_t _e = (expr);                                                                    \
+    if (_e != cudaSuccess) {                                                                    \
+      throw ::pkde::Error{_e == cudaErrorMemoryAllocation ? PKDE_ENOMEM : PKDE_ECUDA,          \
+                          std::string(#expr) + ": " + cudaGetErrorString(_e)};                  \
+    }                                                                                           \
+  } while (0)
+
+#define PKDE_CHECK_LAUNCH() PKDE_CUDA_TRY(cudaGetLastError())
+
+inline Error invalid(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  return Error{PKDE_EINVAL, buf};
+}
+
+// ------------------------------------------------------------------------ device buffer
+// Grow-only device allocation owned by the context; reused across calls.
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t want) {
+    if (want <= bytes) return;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    PKDE_CUDA_TRY(cudaMalloc(&ptr, want));
+    bytes = want;
+  }
+  template <class T>
+  T *as() const {
+    return reinterpret_cast<T *>(ptr);
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+};
+
+enum BufId {
+  BUF_DATA = 0,     // samples (device copy)
+  BUF_IDX,          // bootstrap indices (device copy)
+  BUF_PRE_CELL,     // per-sample lower cell
+  BUF_PRE_RH,       // per-sample remainders
+  BUF_COUNTS,       // per (bootstrap, cell) draw counts
+  BUF_FIX,          // fixed-point accumulators
+  BUF_SPECTRA,      // paired spectra
+  BUF_SCRATCH,      // per-step intermediate
+  BUF_WELFORD,      // per-point Welford state
+  BUF_STATE,        // convergence state
+  BUF_TABLES,       // twiddles, propagation factors, per-step scalars
+  BUF_OUT,          // device copies of outputs
+  BUF_MISC,         // reductions
+  BUF_COUNT_
+};
+
+}  // namespace pkde
+
+struct pkde_ctx {
+  int device = 0;
+  std::string last_error;
+  pkde::DevBuf buf[pkde::BUF_COUNT_];
+  std::map<int, pkde::DevBuf> twiddles;  // per line length
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  // tracing (pkde_set_profiling / pkde_get_stats)
+  bool profiling = false;
+  uint64_t launches = 0;
+  uint64_t phase_launches[PKDE_NPHASES] = {};
+  double phase_ms[PKDE_NPHASES] = {};
+  struct Pending {
+    int phase;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> event_pool;
+};
+
+namespace pkde {
+
+// Launch accounting: call trace_begin before and trace_end after each kernel launch.
+inline cudaEvent_t pooled_event(pkde_ctx *ctx) {
+  if (!ctx->event_pool.empty()) {
+    cudaEvent_t e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+struct Trace {
+  pkde_ctx *ctx;
+  int phase;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+  Trace(pkde_ctx *c, int p, cudaStream_t s) : ctx(c), phase(p), st(s) {
+    ctx->launches++;
+    ctx->phase_launches[p]++;
+    if (ctx->profiling) {
+      a = pooled_event(ctx);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~Trace() {
+    if (a) {
+      cudaEvent_t b = pooled_event(ctx);
+      cudaEventRecord(b, st);
+      ctx->pending.push_back({phase, a, b});
+    }
+  }
+};
+// Fold finished event pairs into phase_ms (call after the stream synchronised).
+inline void collect_trace(pkde_ctx *ctx) {
+  for (auto &p : ctx->pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) ctx->phase_ms[p.phase] += ms;
+    ctx->event_pool.push_back(p.a);
+    ctx->event_pool.push_back(p.b);
+  }
+  ctx->pending.clear();
+}
+
+// ------------------------------------------------------------------------ complex FP64
+struct cplx {
+  double re, im;
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// a * (sign * i)
+__device__ __forceinline__ double2 cmul_si(double2 a, int sign) {
+  return sign > 0 ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+// ------------------------------------------------------------------------------ FFT plan
+constexpr int kMaxStages = 24;
+
+struct FftPlan {
+  int n;
+  int nstages;
+  int radix[kMaxStages];
+};
+
+// Factor n into Stockham stages: radix 8, 4, 2 for the power-of-two part, then 3, 5,
+// 7 and any remaining prime as a generic stage.
+inline FftPlan make_plan(int n) {
+  FftPlan p{};
+  p.n = n;
+  int m = n;
+  const int pref[] = {8, 4, 2, 3, 5, 7};
+  for (int r : pref) {
+    while (m % r == 0) {
+      p.radix[p.nstages++] = r;
+      m /= r;
+    }
+  }
+  for (int q = 11; m > 1 && q * q <= m; q += 2) {
+    while (m % q == 0) {
+      p.radix[p.nstages++] = q;
+      m /= q;
+    }
+  }
+  if (m > 1) p.radix[p.nstages++] = m;
+  return p;
+}
+
+// Twiddle table w[m] = (cos(2 pi m / n), sin(2 pi m / n)), m in [0, n), computed in
+// long double and rounded once.
+inline std::vector<double2> make_twiddles(int n) {
+  std::vector<double2> tw(n);
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < n; ++m) {
+    long double a = two_pi * (long double)m / (long double)n;
+    tw[m] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  return tw;
+}
+
+// -------------------------------------------------------------- radix-R butterflies
+// DFT of R values in place: X[q] = sum_r v[r] exp(DIR * 2 pi i q r / R).
+template <int DIR>
+__device__ __forceinline__ void dft2(double2 *v) {
+  double2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft4(double2 *v) {
+  double2 t0 = cadd(v[0], v[2]);
+  double2 t1 = csub(v[0], v[2]);
+  double2 t2 = cadd(v[1], v[3]);
+  double2 t3 = cmul_si(csub(v[1], v[3]), DIR);
+  v[0] = cadd(t0, t2);
+  v[2] = csub(t0, t2);
+  v[1] = cadd(t1, t3);
+  v[3] = csub(t1, t3);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft8(double2 *v) {
+  const double h = 0.70710678118654752440;  // sqrt(1/2)
+  double2 e[4] = {v[0], v[2], v[4], v[6]};
+  double2 o[4] = {v[1], v[3], v[5], v[7]};
+  dft4<DIR>(e);
+  dft4<DIR>(o);
+  // W8^k, W8 = exp(DIR * 2 pi i / 8)
+  double2 o1 = make_double2(h * (o[1].x - DIR * o[1].y), h * (o[1].y + DIR * o[1].x));
+  double2 o2 = cmul_si(o[2], DIR);
+  double2 o3 = make_double2(h * (-o[3].x - DIR * o[3].y), h * (-o[3].y + DIR * o[3].x));
+  v[0] = cadd(e[0], o[0]);
+  v[4] = csub(e[0], o[0]);
+  v[1] = cadd(e[1], o1);
+  v[5] = csub(e[1], o1);
+  v[2] = cadd(e[2], o2);
+  v[6] = csub(e[2], o2);
+  v[3] = cadd(e[3], o3);
+  v[7] = csub(e[3], o3);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft3(double2 *v) {
+  const double s3 = 0.86602540378443864676;  // sin(2 pi / 3)
+  double2 t = cadd(v[1], v[2]);
+  double2 d = csub(v[1], v[2]);
+  double2 m = make_double2(v[0].x - 0.5 * t.x, v[0].y - 0.5 * t.y);
+  double2 rot = cmul_si(cscale(d, s3), DIR);
+  v[0] = cadd(v[0], t);
+  v[1] = cadd(m, rot);
+  v[2] = csub(m, rot);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft5(double2 *v) {
+  const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+  const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+  double2 a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+  double2 a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+  double2 x0 = v[0];
+  double2 p1 = make_double2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+  double2 p2 = make_double2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+  double2 q1 = cmul_si(make_double2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y), DIR);
+  double2 q2 = cmul_si(make_double2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y), DIR);
+  v[0] = cadd(x0, cadd(a1, a2));
+  v[1] = cadd(p1, q1);
+  v[4] = csub(p1, q1);
+  v[2] = cadd(p2, q2);
+  v[3] = csub(p2, q2);
+}
+
+__device__ __forceinline__ double2 twiddle(const double2 *tw, int m, int dir) {
+  double2 w = tw[m];
+  return make_double2(w.x, dir * w.y);
+}
+
+// One Stockham stage of radix R over `nlines` lines held in shared memory
+// (line pitch `pitch` complex values).  src -> dst.
+template <int DIR, int R>
+__device__ __forceinline__ void stockham_stage(const double2 *src, double2 *dst, int n, int pitch,
+                                               int nlines, int Ns, const double2 *tw) {
+  const int nb = n / R;
+  const int tstep = n / (Ns * R);
+  for (int t = threadIdx.x; t < nlines * nb; t += blockDim.x) {
+    const int l = t / nb;
+    const int j = t - l * nb;
+    const int k = j % Ns;
+    const double2 *s = src + l * pitch;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      double2 x = s[j + r * nb];
+      if (r > 0 && k > 0) x = cmul(x, twiddle(tw, r * k * tstep, DIR));
+      v[r] = x;
+    }
+    if constexpr (R == 2) dft2<DIR>(v);
+    if constexpr (R == 4) dft4<DIR>(v);
+    if constexpr (R == 8) dft8<DIR>(v);
+    if constexpr (R == 3) dft3<DIR>(v);
+    if constexpr (R == 5) dft5<DIR>(v);
+    const int d = (j / Ns) * Ns * R + k;
+    double2 *o = dst + l * pitch;
+#pragma unroll
+    for (int q = 0; q < R; ++q) o[d + q * Ns] = v[q];
+  }
+}
+
+// Generic radix (any R): one thread per output value, O(R) work each.
+template <int DIR>
+__device__ __forceinline__ void stockham_stage_generic(const double2 *src, double2 *dst, int n,
+                                                       int pitch, int nlines, int Ns, int R,
+                                                       const double2 *tw) {
+  const int nb = n / R;
+  const int tstep = n / (Ns * R);
+  for (int t = threadIdx.x; t < nlines * n; t += blockDim.x) {
+    const int l = t / n;
+    const int u = t - l * n;
+    const int j = u / R;
+    const int q = u - j * R;
+    const int k = j % Ns;
+    const double2 *s = src + l * pitch;
+    const int base = k * tstep + q * nb;  // exponent per input index r
+    double2 acc = make_double2(0.0, 0.0);
+    int m = 0;
+    for (int r = 0; r < R; ++r) {
+      double2 x = s[j + r * nb];
+      double2 w = twiddle(tw, m, DIR);
+      acc.x += x.x * w.x - x.y * w.y;
+      acc.y += x.x * w.y + x.y * w.x;
+      m += base;
+      if (m >= n) m -= n;
+    }
+    const int d = (j / Ns) * Ns * R + k;
+    dst[l * pitch + d + q * Ns] = acc;
+  }
+}
+
+// Full FFT of `nlines` lines in shared memory.  Data starts in bufA; returns the
+// buffer holding the result (bufA or bufB).  Ends with __syncthreads().
+template <int DIR>
+__device__ double2 *smem_fft(double2 *bufA, double2 *bufB, int pitch, int nlines, const FftPlan &plan,
+                             const double2 *tw) {
+  double2 *src = bufA, *dst = bufB;
+  int Ns = 1;
+  const int n = plan.n;
+  for (int st = 0; st < plan.nstages; ++st) {
+    const int R = plan.radix[st];
+    switch (R) {
+      case 8: stockham_stage<DIR, 8>(src, dst, n, pitch, nlines, Ns, tw); break;
+      case 4: stockham_stage<DIR, 4>(src, dst, n, pitch, nlines, Ns, tw); break;
+      case 2: stockham_stage<DIR, 2>(src, dst, n, pitch, nlines, Ns, tw); break;
+      case 3: stockham_stage<DIR, 3>(src, dst, n, pitch, nlines, Ns, tw); break;
+      case 5: stockham_stage<DIR, 5>(src, dst, n, pitch, nlines, Ns, tw); break;
+      default: stockham_stage_generic<DIR>(src, dst, n, pitch, nlines, Ns, R, tw); break;
+    }
+    __syncthreads();
+    double2 *tmp = src;
+    src = dst;
+    dst = tmp;
+    Ns *= R;
+  }
+  return src;
+}
+
+// Lines along one grid axis of a batch of complex arrays:
+// line L -> (array a, outer o, inner i); element k at a*array_stride + (o*n + k)*inner + i.
+struct LineSet {
+  int n;
+  int64_t inner;
+  int64_t outer;
+  int64_t arrays;
+  int64_t array_stride;
+  __host__ __device__ int64_t nlines() const { return arrays * outer * inner; }
+  __host__ __device__ int64_t base(int64_t L) const {
+    int64_t i = L % inner;
+    int64_t r = L / inner;
+    int64_t o = r % outer;
+    int64_t a = r / outer;
+    return a * array_stride + o * (int64_t)n * inner + i;
+  }
+};
+
+inline LineSet axis_lines(int ndim, const int64_t *dims, int axis, int64_t arrays) {
+  LineSet ls{};
+  ls.n = (int)dims[axis];
+  int64_t inner = 1, outer = 1, G = 1;
+  for (int j = 0; j < ndim; ++j) G *= dims[j];
+  for (int j = 0; j < axis; ++j) inner *= dims[j];
+  for (int j = axis + 1; j < ndim; ++j) outer *= dims[j];
+  ls.inner = inner;
+  ls.outer = outer;
+  ls.arrays = arrays;
+  ls.array_stride = G;
+  return ls;
+}
+
+// The bootstrap draw of the counter-based generator (0-based); see pkde_b200.h.
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__host__ __device__ __forceinline__ int64_t boot_draw(uint64_t seed, int64_t n, int64_t b, int64_t j) {
+  uint64_t x = seed + (uint64_t)(b * n + j + 1) * 0x9E3779B97F4A7C15ull;
+  uint64_t z = splitmix64(x);
+  return (int64_t)(((z >> 32) * (uint64_t)n) >> 32);
+}
+
+// ---------------------------------------------------------------- host-side helpers
+int grid_validate(const pkde_grid *g);
+int64_t grid_size(const pkde_grid *g);
+void *ensure(pkde_ctx *ctx, BufId id, size_t bytes);
+void copy_in(void *dst, const void *src, size_t bytes, bool src_on_device, cudaStream_t st);
+void copy_out(void *dst, const void *src, size_t bytes, bool dst_on_device, cudaStream_t st);
+
+// FFT driver (pkde_fft.cu): in-place N-D transform of `batch` complex arrays.
+void fft_nd(pkde_ctx *ctx, int ndim, const int64_t *dims, double2 *data, int64_t batch, int dir,
+            cudaStream_t st, int phase);
+// Device twiddle table for size n (cached per context).
+const double2 *twiddles_device(pkde_ctx *ctx, int n);
+// Launch one axis pass: out[line] = FFT_dir(in[line] * factor), factor per element k of the
+// axis taken from factors[a % nfac][k] * scal[a % nfac] (factors may be null).
+void fft_axis(pkde_ctx *ctx, const LineSet &ls, const double2 *in, double2 *out, int dir,
+              const double *const *factors, const double *scal, int nfac, cudaStream_t st, int phase);
+
+// binning (pkde_binning.cu): fills spectra-ready FP64 arrays
+struct BinResult {
+  double *means;   // G x nb
+  double *sq;      // G x nb (null if not requested)
+  uint32_t *counts;
+};
+void dirac_device(pkde_ctx *ctx, const pkde_grid *g, const double *d_data, int64_t n,
+                  const int32_t *d_idx, int64_t nboot, bool identity, uint64_t seed, double *d_means,
+                  double *d_sq, uint32_t *d_counts, cudaStream_t st);
+
+}  // namespace pkde
+
+// Entry-point wrapper: converts exceptions into status codes + last_error.
+template <class F>
+static int pkde_guard(pkde_ctx *ctx, F &&f) {
+  try {
+    f();
+    return PKDE_OK;
+  } catch (const pkde::Error &e) {
+    if (ctx) ctx->last_error = e.msg;
+    return e.code;
+  } catch (const std::exception &e) {
+    if (ctx) ctx->last_error = e.what();
+    return PKDE_ECUDA;
+  }
+}
