@@ -167,9 +167,14 @@ def main():
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--bandwidth-steps", type=int, default=None,
+                    help="override the workload's bandwidth steps (small profiling runs only)")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
     x, gspec, kw = workload(args.workload)
+    if args.bandwidth_steps:
+        kw["n_steps"] = args.bandwidth_steps
     wl_name = {"c1": "1-D N(0,1) n=1e4, 1024 pts, B=100, 251 bandwidths",
                "c2": "2-D 3-GMM n=1e6, 512x512, B=64, 201 bandwidths",
                "c3": "3-D banana+t3 n=4e6, 128^3, B=32, 151 bandwidths"}[args.workload]
@@ -245,26 +250,28 @@ def main():
     value = units / (t_max / 1000.0)
 
     # e2e through the public API with page-locked host samples
-    est = pk.initialize_estimation(x, grid=grid)
-    est.kde.pin()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    e0 = time.perf_counter()
-    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev2.record(stream)
-    for k in range(args.steps):
-        pk.estimate_density(est, "gradepro", n_bootstraps=kw["n_bootstraps"], n_steps=kw["n_steps"],
-                            seed=rank * 100000 + k, device_id=local)
-        pk.get_density(est)
-    ev3.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max(ev2.elapsed_time(ev3), (time.perf_counter() - e0) * 1000.0)
-    if dist:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = units / (e2e_ms / 1000.0)
+    e2e_value = None
+    if not args.no_e2e:
+        est = pk.initialize_estimation(x, grid=grid)
+        est.kde.pin()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0 = time.perf_counter()
+        ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev2.record(stream)
+        for k in range(args.steps):
+            pk.estimate_density(est, "gradepro", n_bootstraps=kw["n_bootstraps"], n_steps=kw["n_steps"],
+                                seed=rank * 100000 + k, device_id=local)
+            pk.get_density(est)
+        ev3.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = max(ev2.elapsed_time(ev3), (time.perf_counter() - e0) * 1000.0)
+        if dist:
+            t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e_value = units / (e2e_ms / 1000.0)
 
     # roofline of the per-bandwidth-step pipeline: FP64 spectra (2 bootstraps' means or
     # second moments per complex array, plus the full-sample means) read once per step:

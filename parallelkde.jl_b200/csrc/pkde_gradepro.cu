@@ -19,6 +19,7 @@
 #include <limits>
 
 #include "pkde_internal.cuh"
+#include "pkde_step.cuh"
 
 namespace pkde {
 
@@ -31,51 +32,11 @@ namespace {
 constexpr int kThreads = 256;
 
 // ------------------------------------------------------------------- convergence
-struct StepResult {
-  bool more_stable;
-  double new_min;
-  uint16_t c_low, c_over;
-  uint8_t flag;
-};
-
-// find_stability (DirectSpace.jl:975-1031) with first/second_difference (:1092-1100).
-__device__ __forceinline__ StepResult find_stability(double f, double f1, double f2, double dlogt, double eps,
-                                                     int64_t steps_low, int64_t steps_over, double minimum,
-                                                     uint16_t c_low, uint16_t c_over, uint8_t flag) {
-  const double d1 = log(fabs(__ddiv_rn(__dsub_rn(f, f1), __dmul_rn(2.0, dlogt))));
-  const double d2 = log(fabs(__ddiv_rn(__dadd_rn(__dsub_rn(f, __dmul_rn(2.0, f1)), f2), __dmul_rn(dlogt, dlogt))));
-  StepResult r{false, nan(""), c_low, c_over, flag};
-  if (!flag) {
-    if (d2 < eps) {
-      if (((d1 < minimum) || isnan(minimum)) && ((int64_t)c_over <= steps_over)) {
-        r.more_stable = true;
-        r.new_min = d1;
-        r.c_over = 0;
-      } else {
-        r.c_over = (uint16_t)(c_over + 1);
-      }
-    } else {
-      r.c_low = (uint16_t)(c_low + 1);
-      if ((int64_t)r.c_low > steps_low) {
-        r.flag = 1;
-        minimum = nan("");
-      }
-    }
-  } else {
-    if ((d2 < eps) && isnan(minimum)) {
-      r.more_stable = true;
-      r.new_min = d1;
-    }
-  }
-  if (isnan(r.new_min)) r.new_min = minimum;
-  return r;
-}
-
 __global__ void converge_kernel(int64_t G, double *density, const double *means, const double *f, const double *f1,
                                 const double *f2, double dlogt, double eps, int64_t steps_low, int64_t steps_over,
                                 double *minima, uint16_t *c_low, uint16_t *c_over, uint8_t *flags) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < G; i += (int64_t)gridDim.x * blockDim.x) {
-    StepResult r = find_stability(f[i], f1[i], f2[i], dlogt, eps, steps_low, steps_over, minima[i], c_low[i],
+    StabilityResult r = find_stability(f[i], f1[i], f2[i], dlogt, eps, steps_low, steps_over, minima[i], c_low[i],
                                   c_over[i], flags[i]);
     c_low[i] = r.c_low;
     c_over[i] = r.c_over;
@@ -187,16 +148,11 @@ __global__ void __launch_bounds__(kThreads) vmr_axis1_kernel(
   }
 }
 
-struct ConvState {
-  double *f1, *f2, *minima, *density, *mu_last;
-  uint16_t *c_low, *c_over;
-  uint8_t *flags;
-  int32_t *selected;
-};
+using ConvState = StepState;
 
 // Means of the full sample (DirectSpace.jl:747-764) for one step, the scaled VMR
 // variance from the Welford state (:579-580), and the convergence update
-// (GradeProEstimator.jl:638-669).
+// (GradeProEstimator.jl:638-669).  Generic line lengths.
 template <int PPT>
 __global__ void __launch_bounds__(kThreads) means_converge_kernel(
     const double2 *__restrict__ in, int n1, int64_t rows, FftPlan plan, const double2 *__restrict__ tw,
@@ -219,22 +175,7 @@ __global__ void __launch_bounds__(kThreads) means_converge_kernel(
     const int64_t i = r0 * n1 + e;
     const double2 z = res[(e / n1) * pitch + (e % n1)];
     const double mu = sqrt(__dadd_rn(__dmul_rn(z.x, z.x), __dmul_rn(z.y, z.y)));
-    const double v = __ddiv_rn(__dmul_rn(vscale, wm2[i]), bm1);
-    const double f = isfinite(v) ? log(v) : nan("");
-    const double f1 = cs.f1[i], f2 = cs.f2[i];
-    StepResult r = find_stability(f, f1, f2, dlogt, eps, steps_low, steps_over, cs.minima[i], cs.c_low[i],
-                                  cs.c_over[i], cs.flags[i]);
-    cs.c_low[i] = r.c_low;
-    cs.c_over[i] = r.c_over;
-    cs.flags[i] = r.flag;
-    cs.minima[i] = r.new_min;
-    if (r.more_stable) {
-      cs.density[i] = mu;
-      cs.selected[i] = step;
-    }
-    cs.f2[i] = f1;
-    cs.f1[i] = f;
-    cs.mu_last[i] = mu;
+    step_update(cs, i, mu, __ddiv_rn(__dmul_rn(vscale, wm2[i]), bm1), dlogt, eps, steps_low, steps_over, step);
   }
 }
 
@@ -587,6 +528,8 @@ void run_gradepro(pkde_ctx *ctx, const Estimation &E, double *d_density, int32_t
     throw Error{PKDE_EUNSUPPORTED, "grid axis 1 too long"};
   };
 
+  const bool pow2 = N > 1 && pow2_path_ok(g);
+  const double inv_n = 1.0 / nsd;
   for (int64_t s = 0; s < L.S; ++s) {
     const double *fzs = dfz + s * tot, *fws = dfw + s * tot;
     for (int64_t p0 = 0; p0 < npairs; p0 += group) {
@@ -598,11 +541,18 @@ void run_gradepro(pkde_ctx *ctx, const Estimation &E, double *d_density, int32_t
           LineSet ls = axis_lines(N, g->dims, a, 2 * np);
           const double *facs[2] = {fzs + aoff[a], fws + aoff[a]};
           const double ones[2] = {1.0, 1.0};
-          fft_axis(ctx, ls, a == N - 1 ? src : scratch, scratch, 1, facs, ones, 2, st, PKDE_PHASE_STEP_FFT);
+          if (pow2)
+            axis_pass_pow2(ctx, ls, a == N - 1 ? src : scratch, scratch, facs, ones, 2, st);
+          else
+            fft_axis(ctx, ls, a == N - 1 ? src : scratch, scratch, 1, facs, ones, 2, st, PKDE_PHASE_STEP_FFT);
         }
         src = scratch;
       }
-      launch_vmr(src, np, (int)(2 * p0), p0 == 0 ? 1 : 0, fzs + aoff[0], fws + aoff[0], invG, invG * L.cw[s]);
+      if (pow2)
+        vmr_pass_pow2(ctx, n1, src, np, (int)(2 * p0), (int)B, rows, fzs + aoff[0], fws + aoff[0], invG,
+                      invG * L.cw[s], inv_n, G, wel, p0 == 0 ? 1 : 0, st);
+      else
+        launch_vmr(src, np, (int)(2 * p0), p0 == 0 ? 1 : 0, fzs + aoff[0], fws + aoff[0], invG, invG * L.cw[s]);
     }
     const double2 *msrc = spectra + 2 * npairs * G;
     if (N > 1) {
@@ -610,11 +560,18 @@ void run_gradepro(pkde_ctx *ctx, const Estimation &E, double *d_density, int32_t
         LineSet ls = axis_lines(N, g->dims, a, 1);
         const double *facs[1] = {fzs + aoff[a]};
         const double ones[1] = {1.0};
-        fft_axis(ctx, ls, a == N - 1 ? msrc : scratch, scratch, 1, facs, ones, 1, st, PKDE_PHASE_STEP_FFT);
+        if (pow2)
+          axis_pass_pow2(ctx, ls, a == N - 1 ? msrc : scratch, scratch, facs, ones, 1, st);
+        else
+          fft_axis(ctx, ls, a == N - 1 ? msrc : scratch, scratch, 1, facs, ones, 1, st, PKDE_PHASE_STEP_FFT);
       }
       msrc = scratch;
     }
-    launch_means(msrc, fzs + aoff[0], invG, s);
+    if (pow2)
+      means_pass_pow2(ctx, n1, msrc, rows, fzs + aoff[0], invG, wel, G, (int)B, L.vscale[s], L.dlogt[s], L.eps,
+                      L.steps_low, L.steps_over, cs, (int)s, st);
+    else
+      launch_means(msrc, fzs + aoff[0], invG, s);
   }
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);

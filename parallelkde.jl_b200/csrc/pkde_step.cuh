@@ -1,0 +1,90 @@
+// Per-grid-point convergence state and the step update shared by the step kernels.
+#pragma once
+
+#include "pkde_internal.cuh"
+
+namespace pkde {
+
+// Convergence state of every grid point (DensityState, GradeProEstimator.jl:515-615),
+// plus the outputs: density, selected step, and the last step's means.
+struct StepState {
+  double *f1, *f2, *minima, *density, *mu_last;
+  uint16_t *c_low, *c_over;
+  uint8_t *flags;
+  int32_t *selected;
+};
+
+struct StabilityResult {
+  bool more_stable;
+  double new_min;
+  uint16_t c_low, c_over;
+  uint8_t flag;
+};
+
+// find_stability (DirectSpace.jl:975-1031) with first/second_difference (:1092-1100),
+// in FP64.  Explicit-rounding intrinsics keep the operation order of the reference.
+__device__ __forceinline__ StabilityResult find_stability(double f, double f1, double f2, double dlogt, double eps,
+                                                          int64_t steps_low, int64_t steps_over, double minimum,
+                                                          uint16_t c_low, uint16_t c_over, uint8_t flag) {
+  const double d1 = log(fabs(__ddiv_rn(__dsub_rn(f, f1), __dmul_rn(2.0, dlogt))));
+  const double d2 = log(fabs(__ddiv_rn(__dadd_rn(__dsub_rn(f, __dmul_rn(2.0, f1)), f2), __dmul_rn(dlogt, dlogt))));
+  StabilityResult r{false, nan(""), c_low, c_over, flag};
+  if (!flag) {
+    if (d2 < eps) {
+      if (((d1 < minimum) || isnan(minimum)) && ((int64_t)c_over <= steps_over)) {
+        r.more_stable = true;
+        r.new_min = d1;
+        r.c_over = 0;
+      } else {
+        r.c_over = (uint16_t)(c_over + 1);
+      }
+    } else {
+      r.c_low = (uint16_t)(c_low + 1);
+      if ((int64_t)r.c_low > steps_low) {
+        r.flag = 1;
+        minimum = nan("");
+      }
+    }
+  } else {
+    if ((d2 < eps) && isnan(minimum)) {
+      r.more_stable = true;
+      r.new_min = d1;
+    }
+  }
+  if (isnan(r.new_min)) r.new_min = minimum;
+  return r;
+}
+
+// One step of update_state! (GradeProEstimator.jl:638-669) at grid point i:
+// v = scaled bootstrap variance of the VMR (DirectSpace.jl:579), mu = the means.
+__device__ __forceinline__ void step_update(const StepState &cs, int64_t i, double mu, double v, double dlogt,
+                                            double eps, int64_t steps_low, int64_t steps_over, int step) {
+  const double f = isfinite(v) ? log(v) : nan("");
+  const double f1 = cs.f1[i], f2 = cs.f2[i];
+  StabilityResult r = find_stability(f, f1, f2, dlogt, eps, steps_low, steps_over, cs.minima[i], cs.c_low[i],
+                                     cs.c_over[i], cs.flags[i]);
+  cs.c_low[i] = r.c_low;
+  cs.c_over[i] = r.c_over;
+  cs.flags[i] = r.flag;
+  cs.minima[i] = r.new_min;
+  if (r.more_stable) {
+    cs.density[i] = mu;
+    cs.selected[i] = step;
+  }
+  cs.f2[i] = f1;
+  cs.f1[i] = f;
+  cs.mu_last[i] = mu;
+}
+
+// power-of-two path (pkde_step.cu)
+bool pow2_path_ok(const pkde_grid *g);
+void axis_pass_pow2(pkde_ctx *ctx, const LineSet &ls, const double2 *in, double2 *out, const double *const *factors,
+                    const double *scal, int nfac, cudaStream_t st);
+void vmr_pass_pow2(pkde_ctx *ctx, int n1, const double2 *in, int npairs, int b0, int nboot, int64_t rows,
+                   const double *fz, const double *fw, double cz, double cw, double inv_n, int64_t G, double *wstate,
+                   int first, cudaStream_t st);
+void means_pass_pow2(pkde_ctx *ctx, int n1, const double2 *in, int64_t rows, const double *fz, double cz,
+                     const double *wstate, int64_t G, int nboot, double vscale, double dlogt, double eps,
+                     int64_t steps_low, int64_t steps_over, const StepState &cs, int step, cudaStream_t st);
+
+}  // namespace pkde

@@ -147,11 +147,13 @@ class Parity:
               f"rel L2 {self.rel_stable:.2e}")
 
     def check(self):
-        # exact agreement wherever the reference's own outcome is rounding-independent
-        assert self.agree_stable >= 0.999
+        G = self.sel.size
+        # identical densities wherever the selected step agrees (FP64 round-off only)
         assert self.rel_stable <= 1e-10
-        # no more noise-decided flips than a second FP64 implementation shows (+ slack)
-        assert self.flips <= 2 * self.flips_alt + 2
+        # the GPU flips no more decisions than a second FP64 implementation of the
+        # reference does (decisions within round-off of the threshold are coin flips)
+        assert self.flips <= 1.5 * self.flips_alt + 0.001 * G + 2
+        assert self.agree_stable >= 1.0 - 3.0 * (1.0 - self.agree_alt) - 0.001
 
 
 def _compare(pk, oracle, data, og_grid, B, n_steps=None, idx_seed=5, **kw):
@@ -166,7 +168,10 @@ def _compare(pk, oracle, data, og_grid, B, n_steps=None, idx_seed=5, **kw):
 
 
 @pytest.mark.parametrize("n_dims,dims,n,B,steps", [(1, (256,), 4000, 10, 60), (2, (48, 40), 20000, 8, 50),
-                                                   (3, (16, 20, 12), 20000, 6, 30), (4, (8, 6, 10, 7), 20000, 4, 20)])
+                                                   (3, (16, 20, 12), 20000, 6, 30), (4, (8, 6, 10, 7), 20000, 4, 20),
+                                                   (2, (64, 32), 20000, 8, 40), (2, (256, 128), 50000, 5, 30),
+                                                   (3, (16, 32, 16), 20000, 6, 30), (2, (2048, 16), 20000, 4, 20),
+                                                   (4, (16, 16, 16, 16), 30000, 4, 12)])
 def test_estimate_matches_oracle(pk, oracle, n_dims, dims, n, B, steps):
     rng = np.random.default_rng(10 + n_dims)
     data = rng.standard_normal((n_dims, n))
