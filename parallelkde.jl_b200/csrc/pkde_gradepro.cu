@@ -470,11 +470,62 @@ void run_gradepro(pkde_ctx *ctx, const Estimation &E, double *d_density, int32_t
   dirac_paired(ctx, g, E.d_data, E.n, E.d_idx, B, E.seed, spectra, st);
   fft_nd(ctx, N, g->dims, spectra, 2 * npairs + 1, -1, st, PKDE_PHASE_FORWARD_FFT);
 
+  if (steps1d_ok(g)) {
+    // 1-D: every bandwidth step in parallel (one CTA each), then the convergence
+    // state machine over the stored per-step f_s and means.
+    const int64_t S = L.S;
+    double *per_step = (double *)ensure(ctx, BUF_SCRATCH, sizeof(double) * (2 * S * G + 3 * S));
+    double *f_all = per_step, *mu_all = per_step + S * G;
+    double *d_cw = mu_all + S * G, *d_vs = d_cw + S, *d_dl = d_vs + S;
+    PKDE_CUDA_TRY(cudaMemcpyAsync(d_cw, L.cw.data(), sizeof(double) * S, cudaMemcpyHostToDevice, st));
+    PKDE_CUDA_TRY(cudaMemcpyAsync(d_vs, L.vscale.data(), sizeof(double) * S, cudaMemcpyHostToDevice, st));
+    PKDE_CUDA_TRY(cudaMemcpyAsync(d_dl, L.dlogt.data(), sizeof(double) * S, cudaMemcpyHostToDevice, st));
+    steps1d(ctx, n1, spectra, (int)npairs, (int)B, (int)S, dfz, dfw, tot, d_cw, 1.0 / (double)G, 1.0 / (double)E.n,
+            d_vs, f_all, mu_all, st);
+    converge_steps(ctx, G, (int)S, f_all, mu_all, d_dl, L.eps, L.steps_low, L.steps_over, cs, st);
+    if (d_density) PKDE_CUDA_TRY(cudaMemcpyAsync(d_density, cs.density, sizeof(double) * G, cudaMemcpyDeviceToDevice, st));
+    if (d_selected)
+      PKDE_CUDA_TRY(cudaMemcpyAsync(d_selected, cs.selected, sizeof(int32_t) * G, cudaMemcpyDeviceToDevice, st));
+    return;
+  }
+
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
     init_state_kernel<<<blocks_for(ctx, G), kThreads, 0, st>>>(G, cs);
   }
   PKDE_CHECK_LAUNCH();
+
+  if (engine_ok(g)) {
+    // N-D on power-of-two axes: the persistent step engine runs every bandwidth step
+    EngineArgs A{};
+    A.grid = g;
+    A.npairs = (int)npairs;
+    A.nboot = (int)B;
+    A.S = (int)L.S;
+    A.spectra = spectra;
+    A.fz = dfz;
+    A.fw = dfw;
+    A.tab_stride = tot;
+    for (int j = 0; j < N; ++j) A.aoff[j] = aoff[j];
+    A.cw = L.cw.data();
+    A.vscale = L.vscale.data();
+    A.dlogt = L.dlogt.data();
+    A.inv_n = 1.0 / (double)E.n;
+    A.eps = L.eps;
+    A.steps_low = L.steps_low;
+    A.steps_over = L.steps_over;
+    A.cs = cs;
+    run_engine(ctx, A, st);
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+      replace_nans_kernel<<<blocks_for(ctx, G), kThreads, 0, st>>>(G, cs, (int)L.S);
+    }
+    PKDE_CHECK_LAUNCH();
+    if (d_density) PKDE_CUDA_TRY(cudaMemcpyAsync(d_density, cs.density, sizeof(double) * G, cudaMemcpyDeviceToDevice, st));
+    if (d_selected)
+      PKDE_CUDA_TRY(cudaMemcpyAsync(d_selected, cs.selected, sizeof(int32_t) * G, cudaMemcpyDeviceToDevice, st));
+    return;
+  }
 
   // final-pass geometry
   int tl = std::max(1, std::min<int>(2048 / n1, 16));

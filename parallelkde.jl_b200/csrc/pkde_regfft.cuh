@@ -23,14 +23,16 @@ namespace pkde {
 __host__ __device__ constexpr int pad8(int i) { return i + (i >> 3); }
 __host__ __device__ constexpr int cilog2(int v) { return v <= 1 ? 0 : 1 + cilog2(v >> 1); }
 
-template <int LOGN>
+// Tile geometry for lines of N = 2^LOGN points; NLINES lines per tile (default: enough
+// lines for at least 256 threads).
+template <int LOGN, int NLINES = 0>
 struct Pow2 {
   static constexpr int N = 1 << LOGN;
   static constexpr int NB8 = N / 8;                       // butterflies per line per radix-8 stage
   static constexpr int NST8 = LOGN / 3;                   // radix-8 stages
   static constexpr int REM = LOGN % 3;                    // 1: radix-2 tail, 2: radix-4 tail
-  static constexpr int THREADS = NB8 > 256 ? NB8 : 256;   // one butterfly per thread
-  static constexpr int NL = THREADS / NB8;                // lines per tile
+  static constexpr int NL = NLINES > 0 ? NLINES : (NB8 > 256 ? 1 : 256 / NB8);  // lines per tile
+  static constexpr int THREADS = NL * NB8;                // one butterfly per thread
   static constexpr int LPAD = pad8(N);                    // padded line length before skew
   // skew so that NL lines interleave over the 8 bank groups in COLS mode
   static constexpr int SKEW = NL >= 8 ? 1 : 8 / NL;
@@ -77,9 +79,9 @@ __device__ __forceinline__ double2 twr(const double2 *tw, int i) {
   return make_double2(w.x, DIR > 0 ? w.y : -w.y);
 }
 
-template <int LOGN, bool COLS>
+template <int LOGN, bool COLS, int NLINES = 0>
 struct TileIdx {
-  using P = Pow2<LOGN>;
+  using P = Pow2<LOGN, NLINES>;
   __device__ __forceinline__ static int line() {
     return COLS ? (threadIdx.x & (P::NL - 1)) : (threadIdx.x >> (LOGN - 3));
   }
@@ -196,11 +198,12 @@ __device__ __forceinline__ void run_stages(double2 *line, double2 *v, int t, con
 // FFT of the thread's line.  On entry v[r] = x[in_pos(t, r)]; on exit v[i] =
 // X[out_pos(t, i)].  All threads of the block must call it (it synchronises); the
 // tile memory is free again when it returns.
-template <int LOGN, int DIR, bool COLS>
+template <int LOGN, int DIR, bool COLS, int NLINES = 0>
 __device__ __forceinline__ void tile_fft_reg(double2 *tile, double2 *v, const double2 *tw) {
-  using P = Pow2<LOGN>;
-  double2 *line = tile + TileIdx<LOGN, COLS>::line() * P::LP;
-  run_stages<LOGN, DIR, 0>(line, v, TileIdx<LOGN, COLS>::bfly(), tw);
+  using P = Pow2<LOGN, NLINES>;
+  using I = TileIdx<LOGN, COLS, NLINES>;
+  double2 *line = tile + I::line() * P::LP;
+  run_stages<LOGN, DIR, 0>(line, v, I::bfly(), tw);
 }
 
 }  // namespace pkde

@@ -182,6 +182,75 @@ __global__ void __launch_bounds__(Pow2<LOGN>::THREADS) means_pass_pow2_kernel(
   }
 }
 
+// 1-D grids: one CTA per bandwidth step, the whole line in one tile.  The CTA runs every
+// bootstrap pair (inverse FFT of z and w, VMR, Welford in bootstrap order) and the
+// full-sample means, and stores the step's log scaled variance f_s and means mu_s; the
+// convergence state machine then runs over the steps (converge_steps_kernel).
+template <int LOGN>
+__global__ void __launch_bounds__(Pow2<LOGN, 1>::THREADS) steps1d_kernel(
+    const double2 *__restrict__ spectra, int npairs, int nboot, const double *__restrict__ fz_all,
+    const double *__restrict__ fw_all, int64_t tab_stride, const double *__restrict__ cw, double invG, double inv_n,
+    const double *__restrict__ vscale, const double2 *__restrict__ tw_g, double *__restrict__ f_out,
+    double *__restrict__ mu_out) {
+  using P = Pow2<LOGN, 1>;
+  using I = TileIdx<LOGN, false, 1>;
+  extern __shared__ double2 smem[];
+  double2 *tile = smem;
+  double2 *sm_tw = smem + P::TILE;
+  for (int i = threadIdx.x; i < P::TWSIZE; i += blockDim.x) sm_tw[i] = tw_g[i];
+  const int s = blockIdx.x;
+  const double *fz = fz_all + (int64_t)s * tab_stride;
+  const double *fw = fw_all + (int64_t)s * tab_stride;
+  const double cz_s = invG, cw_s = invG * cw[s];
+  const int t = I::bfly();
+  double mean[8], m2[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) mean[i] = m2[i] = 0.0;
+  __syncthreads();
+  for (int p = 0; p < npairs; ++p) {
+    const double2 *zs = spectra + (int64_t)(2 * p) * P::N;
+    const double2 *ws = zs + P::N;
+    double2 z[8], w[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int k = in_pos<LOGN>(t, r);
+      z[r] = cscale(zs[k], cz_s * fz[k]);
+    }
+    tile_fft_reg<LOGN, 1, false, 1>(tile, z, sm_tw);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int k = in_pos<LOGN>(t, r);
+      w[r] = cscale(ws[k], cw_s * fw[k]);
+    }
+    tile_fft_reg<LOGN, 1, false, 1>(tile, w, sm_tw);
+    const int b = 2 * p;
+    const double inv_a = 1.0 / (double)(b + 1), inv_b = 1.0 / (double)(b + 2);
+    const bool has_b = b + 1 < nboot;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      welford(vmr_of(z[i].x, w[i].x, inv_n), inv_a, mean[i], m2[i]);
+      if (has_b) welford(vmr_of(z[i].y, w[i].y, inv_n), inv_b, mean[i], m2[i]);
+    }
+  }
+  const double2 *zf = spectra + (int64_t)(2 * npairs) * P::N;
+  double2 z[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int k = in_pos<LOGN>(t, r);
+    z[r] = cscale(zf[k], cz_s * fz[k]);
+  }
+  tile_fft_reg<LOGN, 1, false, 1>(tile, z, sm_tw);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int x = out_pos<LOGN>(t, i);
+    const double v = vscale[s] * m2[i] / (double)(nboot - 1);
+    f_out[(int64_t)s * P::N + x] = isfinite(v) ? log(v) : nan("");
+    mu_out[(int64_t)s * P::N + x] = sqrt(z[i].x * z[i].x + z[i].y * z[i].y);
+  }
+}
+
+}  // namespace
+
 const double2 *stage_twiddles_device(pkde_ctx *ctx, int logn) {
   const int key = -logn;  // negative keys: per-stage tables (positive: plain tables)
   auto it = ctx->twiddles.find(key);
@@ -193,6 +262,8 @@ const double2 *stage_twiddles_device(pkde_ctx *ctx, int logn) {
   PKDE_CUDA_TRY(cudaMemcpy(b.ptr, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice));
   return b.as<double2>();
 }
+
+namespace {
 
 template <int LOGN>
 void launch_axis(pkde_ctx *ctx, const LineSet &ls, const double2 *in, double2 *out, const double *const *factors,
@@ -250,9 +321,66 @@ int ilog2_exact(int64_t n) {
   return l;
 }
 
+template <int LOGN>
+void launch_steps1d(pkde_ctx *ctx, const double2 *spectra, int npairs, int nboot, int S, const double *fz_all,
+                    const double *fw_all, int64_t tab_stride, const double *cw, double invG, double inv_n,
+                    const double *vscale, double *f_out, double *mu_out, cudaStream_t st) {
+  using P = Pow2<LOGN, 1>;
+  const size_t smem = sizeof(double2) * ((size_t)P::TILE + P::TWSIZE);
+  PKDE_CUDA_TRY(cudaFuncSetAttribute(steps1d_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const double2 *tw = stage_twiddles_device(ctx, LOGN);
+  {
+    Trace tr(ctx, PKDE_PHASE_STEP_VMR, st);
+    steps1d_kernel<LOGN><<<(unsigned)S, P::THREADS, smem, st>>>(spectra, npairs, nboot, fz_all, fw_all, tab_stride, cw,
+                                                               invG, inv_n, vscale, tw, f_out, mu_out);
+  }
+  PKDE_CHECK_LAUNCH();
+}
+
+__global__ void converge_steps_kernel(int64_t G, int S, const double *__restrict__ f_all,
+                                      const double *__restrict__ mu_all, const double *__restrict__ dlogt, double eps,
+                                      int64_t steps_low, int64_t steps_over, StepState cs) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < G; i += (int64_t)gridDim.x * blockDim.x)
+    converge_point_all_steps(cs, i, G, S, f_all, mu_all, dlogt, eps, steps_low, steps_over);
+}
+
 int lines_per_tile(int logn) { return (1 << logn) / 8 > 256 ? 1 : 256 * 8 / (1 << logn); }
 
 }  // namespace
+
+bool steps1d_ok(const pkde_grid *g) {
+  if (g->ndim != 1) return false;
+  const int ln = ilog2_exact(g->dims[0]);
+  return ln >= 8 && ln <= 12;
+}
+
+void steps1d(pkde_ctx *ctx, int n1, const double2 *spectra, int npairs, int nboot, int S, const double *fz_all,
+             const double *fw_all, int64_t tab_stride, const double *cw, double invG, double inv_n,
+             const double *vscale, double *f_out, double *mu_out, cudaStream_t st) {
+#define PKDE_CALL(L) \
+  launch_steps1d<L>(ctx, spectra, npairs, nboot, S, fz_all, fw_all, tab_stride, cw, invG, inv_n, vscale, f_out, mu_out, st)
+  switch (ilog2_exact(n1)) {
+    case 8: PKDE_CALL(8); break;
+    case 9: PKDE_CALL(9); break;
+    case 10: PKDE_CALL(10); break;
+    case 11: PKDE_CALL(11); break;
+    case 12: PKDE_CALL(12); break;
+    default: throw Error{PKDE_EUNSUPPORTED, "1-D grid length not supported by the step-parallel path"};
+  }
+#undef PKDE_CALL
+}
+
+void converge_steps(pkde_ctx *ctx, int64_t G, int S, const double *f_all, const double *mu_all, const double *dlogt,
+                    double eps, int64_t steps_low, int64_t steps_over, const StepState &cs, cudaStream_t st) {
+  const int threads = 128;
+  const int64_t blocks = std::min<int64_t>((G + threads - 1) / threads, (int64_t)ctx->sm_count * 16);
+  {
+    Trace tr(ctx, PKDE_PHASE_STEP_MEANS, st);
+    converge_steps_kernel<<<(unsigned)blocks, threads, 0, st>>>(G, S, f_all, mu_all, dlogt, eps, steps_low, steps_over,
+                                                                cs);
+  }
+  PKDE_CHECK_LAUNCH();
+}
 
 bool pow2_path_ok(const pkde_grid *g) {
   const int64_t G = grid_size(g);
