@@ -8,7 +8,7 @@
 // N..2 (pass p works on axis N-1-p), then the final axis-1 pass.  A pass is a set of
 // tiles, one tile = one CTA-sized work item.
 //
-// Schedule: round r holds pass p of batch r - p for every p (final passes first), so the
+// Schedule: round r holds pass p of batch r - p*D for every p (final passes first), so the
 // passes of consecutive batches overlap and every dependency points to an earlier
 // round.  CTAs are persistent and take items in this global order from an atomic
 // counter; an item waits (bounded spin) only for items taken before it, so progress is
@@ -58,6 +58,8 @@ struct EngineEst {
   int *cnt;              // NB x P completed tiles per (batch, pass)
   int *fin;              // NB x Tf per-tile final-pass done flags
   int Tf;                // final-pass tiles per batch
+  int tpi[4];            // axis passes: tiles per work item, by axis
+  int D;                 // pass p of batch b runs in round b + p*D
   int *next;             // work counter
   int *error;            // 1: dependency wait timed out
   const double2 *tw[13]; // per-stage twiddle tables by log2(line length)
@@ -97,36 +99,46 @@ __host__ __device__ __forceinline__ int batch_arrays(const EngineEst &E, int64_t
 __host__ __device__ __forceinline__ int pass_tiles(const EngineEst &E, int64_t b, int p) {
   if (p == E.P - 1) return E.Tf;
   const int a = E.ndim - 1 - p;
-  return (int)(batch_arrays(E, b) * (E.G / E.dims[a]) / tile_lines_of(E.logn[a]));
+  return (int)(batch_arrays(E, b) * (E.G / E.dims[a]) / ((int64_t)tile_lines_of(E.logn[a]) * E.tpi[a]));
 }
 
 // ------------------------------------------------------------------ tile bodies
 template <int LOGN>
 __device__ __forceinline__ void stage_tw(double2 *sm_tw, const double2 *tw_g, int &cached, int key) {
-  if (cached != key) {
+  if (cached != key) {  // uniform across the block
+    __syncthreads();
     for (int i = threadIdx.x; i < Pow2<LOGN>::TWSIZE; i += blockDim.x) sm_tw[i] = tw_g[i];
     cached = key;
+    __syncthreads();
   }
-  __syncthreads();
 }
 
-template <int LOGN>
-__device__ void axis_tile(double2 *smem, double2 *sm_tw, const double2 *in, double2 *out, int64_t inner,
-                          int64_t tile_in_array, const double *f) {
+// Inverse FFT of `ntiles` consecutive tiles of NL adjacent lines along an axis >= 2,
+// the axis factor applied on load.  Consecutive lanes take adjacent lines (column
+// mapping), so every global access moves NL*16 contiguous bytes.  FROM_SPECTRA: the
+// input is the read-only spectra, streamed with the evict-first hint so that it does
+// not push the ring slots out of L2; otherwise the input is a ring slot written by
+// other CTAs and is read through L2 only.
+template <int LOGN, bool FROM_SPECTRA>
+__device__ void axis_tiles(double2 *smem, const double2 *sm_tw, const double2 *in, double2 *out, int64_t inner,
+                           int64_t first_tile, int ntiles, const double *f) {
   using P = Pow2<LOGN>;
   using I = TileIdx<LOGN, true>;
-  const int64_t Lw = tile_in_array * P::NL + I::line();
-  const int64_t base = (Lw / inner) * P::N * inner + (Lw % inner);
   const int t = I::bfly();
-  double2 v[8];
+  for (int u = 0; u < ntiles; ++u) {
+    const int64_t Lw = (first_tile + u) * P::NL + I::line();
+    const int64_t base = (Lw / inner) * P::N * inner + (Lw % inner);
+    double2 v[8];
 #pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int k = in_pos<LOGN>(t, r);
-    v[r] = cscale(__ldcg(in + base + (int64_t)k * inner), f[k]);
+    for (int r = 0; r < 8; ++r) {
+      const int k = in_pos<LOGN>(t, r);
+      const double2 x = FROM_SPECTRA ? __ldcs(in + base + (int64_t)k * inner) : __ldcg(in + base + (int64_t)k * inner);
+      v[r] = cscale(x, f[k]);
+    }
+    tile_fft_reg<LOGN, 1, true>(smem, v, sm_tw);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) __stcg(out + base + (int64_t)out_pos<LOGN>(t, i) * inner, v[i]);
   }
-  tile_fft_reg<LOGN, 1, true>(smem, v, sm_tw);
-#pragma unroll
-  for (int i = 0; i < 8; ++i) __stcg(out + base + (int64_t)out_pos<LOGN>(t, i) * inner, v[i]);
 }
 
 __device__ __forceinline__ double div_nr(double v, double m) {
@@ -237,7 +249,7 @@ __device__ bool decode(const EngineEst &E, int64_t item, int64_t &round, Decoded
   if (round >= E.nrounds) return false;
   int64_t off = item - E.round_start[round];
   for (int p = E.P - 1; p >= 0; --p) {
-    const int64_t b = round - p;
+    const int64_t b = round - (int64_t)p * E.D;
     if (b < 0 || b >= E.NB) continue;
     const int n = pass_tiles(E, b, p);
     if (off < n) {
@@ -270,17 +282,20 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineEst E, 
   double2 *tile_mem = smem;
   double2 *state = smem + max_tile;
   double2 *sm_tw = state + 8 * kEngineThreads;
-  __shared__ int64_t s_item;
+  __shared__ int64_t s_next;
   __shared__ int s_ok;
   int cached_tw = -1;
   int64_t round = 0;
   (void)max_tw;
+  // The next item is taken while the current one runs (items are taken in increasing
+  // order per CTA, so every wait still points to an earlier item).
+  if (threadIdx.x == 0) s_next = (int64_t)atomicAdd(E.next, 1);
+  __syncthreads();
+  int64_t item = s_next;
   for (;;) {
-    if (threadIdx.x == 0) s_item = ld_acquire(E.error) ? total_items : (int64_t)atomicAdd(E.next, 1);
-    __syncthreads();
-    const int64_t item = s_item;
-    __syncthreads();
     if (item >= total_items) break;
+    __syncthreads();  // everyone has read s_next
+    if (threadIdx.x == 0) s_next = ld_acquire(E.error) ? total_items : (int64_t)atomicAdd(E.next, 1);
     Decoded d;
     if (!decode(E, item, round, d)) break;
     const int64_t b = d.b;
@@ -316,24 +331,25 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineEst E, 
       const int a = E.ndim - 1 - p;
       const int ln = E.logn[a];
       const int64_t lines = E.G / E.dims[a];
-      const int64_t tpa = lines / tile_lines_of(ln);
-      const int64_t arr = d.tile / tpa;
-      const int64_t tin = d.tile % tpa;
-      const int64_t inner = [&] {
-        int64_t v = 1;
-        for (int q = 0; q < a; ++q) v *= E.dims[q];
-        return v;
-      }();
+      const int tpi = E.tpi[a];
+      const int64_t ipa = lines / ((int64_t)tile_lines_of(ln) * tpi);  // items per array
+      const int64_t arr = d.tile / ipa;
+      const int64_t first_tile = (d.tile % ipa) * tpi;
+      int64_t inner = 1;
+      for (int q = 0; q < a; ++q) inner *= E.dims[q];
       const double2 *in = p == 0 ? (means ? E.spectra + (int64_t)(2 * E.npairs) * E.G
                                           : E.spectra + (int64_t)(2 * j * E.g) * E.G)
                                  : slot_base;
       in += arr * E.G;
       double2 *out = slot_base + arr * E.G;
       const double *f = (!means && (arr & 1)) ? fws + E.aoff[a] : fzs + E.aoff[a];
-#define PKDE_AXIS(L)                                       \
-  {                                                        \
-    stage_tw<L>(sm_tw, E.tw[L], cached_tw, L);             \
-    axis_tile<L>(tile_mem, sm_tw, in, out, inner, tin, f); \
+#define PKDE_AXIS(L)                                                                      \
+  {                                                                                       \
+    stage_tw<L>(sm_tw, E.tw[L], cached_tw, L);                                            \
+    if (p == 0)                                                                           \
+      axis_tiles<L, true>(tile_mem, sm_tw, in, out, inner, first_tile, tpi, f);           \
+    else                                                                                  \
+      axis_tiles<L, false>(tile_mem, sm_tw, in, out, inner, first_tile, tpi, f);          \
   }
       PKDE_ENGINE_SWITCH(ln, PKDE_AXIS)
 #undef PKDE_AXIS
@@ -368,6 +384,7 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineEst E, 
       if (p == E.P - 1) add_release(E.fin + b * E.Tf + d.tile, 1);
       add_release(E.cnt + b * E.P + p, 1);
     }
+    item = s_next;
   }
 }
 
@@ -399,6 +416,14 @@ size_t tw_elems(int logn) {
 }  // namespace
 
 const double2 *stage_twiddles_device(pkde_ctx *ctx, int logn);
+
+// Engine schedule parameters; the environment overrides the defaults (tuning runs).
+int engine_env_int(const char *name, int dflt, int lo, int hi) {
+  const char *v = getenv(name);
+  if (!v || !*v) return dflt;
+  const int x = atoi(v);
+  return x < lo ? lo : (x > hi ? hi : x);
+}
 
 bool engine_ok(const pkde_grid *g) {
   if (g->ndim < 2) return false;
@@ -433,10 +458,19 @@ void run_engine(pkde_ctx *ctx, const EngineArgs &A, cudaStream_t st) {
   const int64_t arr_bytes = (int64_t)sizeof(double2) * E.G;
   E.g = (int)std::max<int64_t>(1, std::min<int64_t>(E.npairs, (16ll << 20) / (2 * arr_bytes)));
   E.J = (E.npairs + E.g - 1) / E.g;
-  E.Q = E.P + 1;
+  // pipeline delay between passes of one batch; ring slots cover the delay
+  E.D = engine_env_int("PKDE_ENGINE_DELAY", 2, 1, 8);
+  E.Q = (E.P - 1) * E.D + 2;
   E.NB = (int64_t)E.S * (E.J + 1);
   E.Tf = (int)((E.G / E.dims[0]) / tile_lines_of(E.logn[0]));
-  E.nrounds = E.NB + E.P - 1;
+  for (int a = 0; a < 4; ++a) E.tpi[a] = 1;
+  for (int a = 1; a < E.ndim; ++a) {
+    const int64_t tiles = (E.G / E.dims[a]) / tile_lines_of(E.logn[a]);
+    int want = engine_env_int("PKDE_ENGINE_TPI", 2, 1, 16);
+    while (want > 1 && tiles % want) want >>= 1;
+    E.tpi[a] = want;
+  }
+  E.nrounds = E.NB + (int64_t)(E.P - 1) * E.D;
   E.slot_elems = (int64_t)2 * E.g * E.G;
   E.spectra = A.spectra;
   E.fz = A.fz;
@@ -460,7 +494,7 @@ void run_engine(pkde_ctx *ctx, const EngineArgs &A, cudaStream_t st) {
   for (int64_t r = 0; r < E.nrounds; ++r) {
     int64_t n = 0;
     for (int p = 0; p < E.P; ++p) {
-      const int64_t b = r - p;
+      const int64_t b = r - (int64_t)p * E.D;
       if (b >= 0 && b < E.NB) n += pass_tiles(E, b, p);
     }
     rs[r + 1] = rs[r] + n;

@@ -73,6 +73,26 @@ inline std::vector<double2> make_stage_twiddles(int logn) {
   return out;
 }
 
+// Synchronisation of the threads that share one line.  In ROWS mapping a line belongs
+// to NB8 consecutive threads: whole warps (named barrier 1 + line, NB8 threads) or a
+// part of one warp (__syncwarp).  In COLS mapping lines interleave across the block,
+// so the whole block synchronises.
+template <int LOGN, bool COLS, int NLINES>
+__device__ __forceinline__ void line_sync(int line) {
+  constexpr int NB8 = Pow2<LOGN, NLINES>::NB8;
+  if constexpr (COLS) {
+    __syncthreads();
+  } else if constexpr (NB8 >= 32) {
+    if constexpr (Pow2<LOGN, NLINES>::NL == 1) {
+      __syncthreads();
+    } else {
+      asm volatile("bar.sync %0, %1;" ::"r"(1 + line), "r"(NB8) : "memory");
+    }
+  } else {
+    __syncwarp();
+  }
+}
+
 template <int DIR>
 __device__ __forceinline__ double2 twr(const double2 *tw, int i) {
   const double2 w = tw[i];
@@ -171,8 +191,8 @@ __device__ __forceinline__ void tail2(double2 *line, double2 *v, int t, const do
   }
 }
 
-template <int LOGN, int DIR, int ST>
-__device__ __forceinline__ void run_stages(double2 *line, double2 *v, int t, const double2 *tw) {
+template <int LOGN, int DIR, int ST, bool COLS, int NLINES>
+__device__ __forceinline__ void run_stages(double2 *line, double2 *v, int t, const double2 *tw, int l) {
   using P = Pow2<LOGN>;
   stage8_compute<LOGN, DIR, ST>(v, t, tw);
   constexpr bool last8 = ST + 1 == P::NST8;
@@ -180,30 +200,30 @@ __device__ __forceinline__ void run_stages(double2 *line, double2 *v, int t, con
     return;  // outputs stay in registers: v[q] = X[t + q*N/8]
   } else {
     stage8_store<LOGN, ST>(line, v, t);
-    __syncthreads();
+    line_sync<LOGN, COLS, NLINES>(l);
     if constexpr (!last8) {
       load8<LOGN>(line, v, t);
-      __syncthreads();
-      run_stages<LOGN, DIR, ST + 1>(line, v, t, tw);
+      line_sync<LOGN, COLS, NLINES>(l);
+      run_stages<LOGN, DIR, ST + 1, COLS, NLINES>(line, v, t, tw, l);
     } else if constexpr (P::REM == 2) {
       tail4<LOGN, DIR>(line, v, t, tw);
-      __syncthreads();
+      line_sync<LOGN, COLS, NLINES>(l);
     } else {
       tail2<LOGN, DIR>(line, v, t, tw);
-      __syncthreads();
+      line_sync<LOGN, COLS, NLINES>(l);
     }
   }
 }
 
 // FFT of the thread's line.  On entry v[r] = x[in_pos(t, r)]; on exit v[i] =
-// X[out_pos(t, i)].  All threads of the block must call it (it synchronises); the
-// tile memory is free again when it returns.
+// X[out_pos(t, i)].  Every thread of the line (COLS: of the block) must call it; the
+// line's tile memory is free again when it returns.
 template <int LOGN, int DIR, bool COLS, int NLINES = 0>
 __device__ __forceinline__ void tile_fft_reg(double2 *tile, double2 *v, const double2 *tw) {
   using P = Pow2<LOGN, NLINES>;
   using I = TileIdx<LOGN, COLS, NLINES>;
-  double2 *line = tile + I::line() * P::LP;
-  run_stages<LOGN, DIR, 0>(line, v, I::bfly(), tw);
+  const int l = I::line();
+  run_stages<LOGN, DIR, 0, COLS, NLINES>(tile + l * P::LP, v, I::bfly(), tw, l);
 }
 
 }  // namespace pkde
