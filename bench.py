@@ -195,7 +195,7 @@ def main():
 
     import torch
     import pkde_b200 as pk
-    from pkde_b200 import _lib, raw
+    from pkde_b200 import _lib, multi, raw
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     pk.load()
@@ -231,7 +231,7 @@ def main():
     for k in range(args.steps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        one(rank * 100000 + k)
+        one(multi.estimation_seed(rank, k))
         b.record(stream)
         lat.append((a, b))
     ev1.record(stream)
@@ -241,11 +241,7 @@ def main():
     stats = _lib.get_stats(local, reset=True)
     elapsed_ms = ev0.elapsed_time(ev1)
     lat_ms = sorted(a.elapsed_time(b) for a, b in lat)
-    t_max = elapsed_ms
-    if dist:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = multi.max_over_ranks(elapsed_ms, dist, dev)
     units = G * S * args.steps * world
     value = units / (t_max / 1000.0)
 
@@ -262,15 +258,12 @@ def main():
         ev2.record(stream)
         for k in range(args.steps):
             pk.estimate_density(est, "gradepro", n_bootstraps=kw["n_bootstraps"], n_steps=kw["n_steps"],
-                                seed=rank * 100000 + k, device_id=local)
+                                seed=multi.estimation_seed(rank, k), device_id=local)
             pk.get_density(est)
         ev3.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max(ev2.elapsed_time(ev3), (time.perf_counter() - e0) * 1000.0)
-        if dist:
-            t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_ms = multi.max_over_ranks(e2e_ms, dist, dev)
         e2e_value = units / (e2e_ms / 1000.0)
 
     # roofline of the per-bandwidth-step pipeline: FP64 spectra (2 bootstraps' means or
