@@ -100,6 +100,21 @@ int pkde_dirac_sequence(pkde_ctx *ctx, const pkde_grid *grid, const double *data
                         const int32_t *boot_idx, int32_t nboot, uint64_t seed, double *means_out,
                         double *sq_out, uint32_t *counts_out, uint32_t flags, void *stream);
 
+/* pkde_dirac_sequence without any device allocation.  No counterpart in the reference.
+ * For callers that cannot allocate device memory: a host framework whose caching
+ * allocator owns the GPU's memory, or a serving loop that must not block in
+ * cudaMalloc/cudaFree, which synchronise the device.  All pointers are device pointers
+ * (means_out required; sq_out, counts_out optional).  Scratch is one fixed array inside
+ * the library (about 9 MB, held by every GPU that loads the library until exit):
+ * at most 16384 samples per call, and when counts_out is NULL at most 2^20 resample x
+ * grid-point counters.  Larger requests return PKDE_EINVAL.  The first call on a device
+ * looks up the array's device address (once per device).  Calls share the array: calls
+ * whose work overlaps on the GPU race; order them on one stream.  ctx may be NULL (it is
+ * used only for the error message). */
+int pkde_dirac_sequence_noalloc(pkde_ctx *ctx, const pkde_grid *grid, const double *data, int64_t n,
+                                const int32_t *boot_idx, int32_t nboot, uint64_t seed, double *means_out,
+                                double *sq_out, uint32_t *counts_out, void *stream);
+
 /* N-D complex FFT of `batch` arrays of G complex values (interleaved re, im FP64).
  * direction -1: forward, unnormalised (fourier_statistics!, FourierSpace.jl:25-104);
  * direction +1: inverse scaled by 1/G (ifourier_statistics!, FourierSpace.jl:445-524). */

@@ -12,6 +12,7 @@
 // rounding of the term values.  Draws are processed bootstrap-major so the atomics of
 // one bootstrap column stay in L2.
 #include <cstring>
+#include <mutex>
 
 #include "pkde_internal.cuh"
 
@@ -373,6 +374,156 @@ extern "C" int pkde_dirac_sequence(pkde_ctx *ctx, const pkde_grid *grid, const d
       else std::memset(sq_out, 0, sizeof(double) * G);
     }
     if (counts_out) copy_out(counts_out, oc, sizeof(uint32_t) * nslots * G, dout, st);
+    PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+  });
+}
+
+// ---------------------------------------------------------------------------------
+// Binning without device allocation (pkde_dirac_sequence_noalloc).
+//
+// For callers that cannot allocate device memory -- a host framework whose caching
+// allocator owns all of the GPU's memory, or a serving loop that must never block in
+// cudaMalloc/cudaFree (both synchronise the device).  Scratch lives in one file-scope
+// device array of fixed size; the caller passes only its input and output buffers.
+// The limits below are the array's capacity.  Every call shares the array and it keeps
+// the last call's contents, so what must start at zero is cleared on each call, and two
+// calls whose work overlaps on the GPU (different streams, or host threads without
+// ordering) race on it.
+// ---------------------------------------------------------------------------------
+namespace pkde {
+namespace {
+
+constexpr int64_t kNoAllocMaxSamples = 16384;     // samples per call
+constexpr int64_t kNoAllocMaxCounts = 1 << 20;    // resamples x grid points, when counts_out is NULL
+constexpr size_t kNoAllocCellBytes = sizeof(uint32_t) * kNoAllocMaxSamples;
+constexpr size_t kNoAllocRhBytes = sizeof(double) * 4 * kNoAllocMaxSamples;
+constexpr size_t kNoAllocQBytes = sizeof(unsigned long long) * 2 * 16 * kNoAllocMaxSamples;
+constexpr size_t kNoAllocCountBytes = sizeof(uint32_t) * kNoAllocMaxCounts;
+constexpr size_t kNoAllocMiscBytes = 256;
+constexpr size_t kNoAllocBytes =
+    kNoAllocCellBytes + kNoAllocRhBytes + kNoAllocQBytes + kNoAllocCountBytes + kNoAllocMiscBytes;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch, looked up once per device (the name is only a
+// host-side stand-in in host code).
+constexpr int kNoAllocMaxDevices = 64;
+unsigned char *g_noalloc_addr[kNoAllocMaxDevices] = {};
+std::mutex g_noalloc_mu;
+
+int noalloc_blocks(int sms, int64_t work) {
+  const int64_t b = (work + kThreads - 1) / kThreads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)sms * 16));
+}
+
+unsigned char *noalloc_scratch_for_current_device() {
+  int dev = 0;
+  PKDE_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) throw invalid("device index %d beyond the supported range", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    PKDE_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = static_cast<unsigned char *>(p);
+  }
+  return g_noalloc_addr[dev];
+}
+
+}  // namespace
+}  // namespace pkde
+
+extern "C" int pkde_dirac_sequence_noalloc(pkde_ctx *ctx, const pkde_grid *grid, const double *data, int64_t n,
+                                           const int32_t *boot_idx, int32_t nboot, uint64_t seed,
+                                           double *means_out, double *sq_out, uint32_t *counts_out, void *stream) {
+  return pkde_guard(ctx, [&] {
+    using namespace pkde;
+    grid_validate(grid);
+    if (!data || !means_out) throw invalid("data and means_out are required (device pointers)");
+    if (nboot < 0) throw invalid("Number of bootstraps must be non-negative");
+    if (n < 1 || n > kNoAllocMaxSamples)
+      throw invalid("pkde_dirac_sequence_noalloc: %lld samples, the limit is %lld", (long long)n,
+                    (long long)kNoAllocMaxSamples);
+    const int N = grid->ndim;
+    const int nc = 1 << N;
+    const int64_t G = grid_size(grid);
+    const bool identity = nboot == 0;
+    const int64_t nb = identity ? 0 : nboot;
+    const int64_t nslots = identity ? 1 : nb;
+    if (!counts_out && nslots * G > kNoAllocMaxCounts)
+      throw invalid("pkde_dirac_sequence_noalloc: %lld resample x grid counters exceed the limit %lld (pass counts_out)",
+                    (long long)(nslots * G), (long long)kNoAllocMaxCounts);
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned char *base = noalloc_scratch_for_current_device();
+    int dev = 0, sms = 1;
+    PKDE_CUDA_TRY(cudaGetDevice(&dev));
+    PKDE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    uint32_t *cell = reinterpret_cast<uint32_t *>(base);
+    double *rh = reinterpret_cast<double *>(base + kNoAllocCellBytes);
+    unsigned long long *qm = reinterpret_cast<unsigned long long *>(base + kNoAllocCellBytes + kNoAllocRhBytes);
+    unsigned long long *qv = qm + (int64_t)16 * kNoAllocMaxSamples;
+    uint32_t *counts = counts_out ? counts_out
+                                  : reinterpret_cast<uint32_t *>(base + kNoAllocCellBytes + kNoAllocRhBytes +
+                                                                 kNoAllocQBytes);
+    int *misc = reinterpret_cast<int *>(base + kNoAllocCellBytes + kNoAllocRhBytes + kNoAllocQBytes +
+                                        kNoAllocCountBytes);
+    int *err = misc;
+    unsigned int *maxc = reinterpret_cast<unsigned int *>(misc + 1);
+    int64_t *corner_off = reinterpret_cast<int64_t *>(misc + 8);
+    GridDev gd = to_dev(grid);
+    int64_t off_h[16];
+    for (int c = 0; c < nc; ++c) {
+      int64_t o = 0;
+      for (int j = 0; j < N; ++j)
+        if (!((c >> (N - 1 - j)) & 1)) o += gd.stride[j];
+      off_h[c] = o;
+    }
+    // scratch keeps the previous call's contents: clear what must start at zero
+    PKDE_CUDA_TRY(cudaMemsetAsync(misc, 0, 64, st));
+    PKDE_CUDA_TRY(cudaMemcpyAsync(corner_off, off_h, sizeof(int64_t) * nc, cudaMemcpyHostToDevice, st));
+    PKDE_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(uint32_t) * nslots * G, st));
+    const unsigned nblk = (unsigned)((n + kThreads - 1) / kThreads);
+    prepass_kernel<<<nblk, kThreads, 0, st>>>(gd, data, n, cell, rh, err);
+    PKDE_CHECK_LAUNCH();
+    count_kernel<<<noalloc_blocks(sms, nslots * n), kThreads, 0, st>>>(cell, n, nslots, nb, G, boot_idx,
+                                                                                      seed, counts, err);
+    PKDE_CHECK_LAUNCH();
+    max_kernel<<<noalloc_blocks(sms, nslots * G), kThreads, 0, st>>>(counts, nslots * G, maxc);
+    PKDE_CHECK_LAUNCH();
+    int hbuf[2];
+    PKDE_CUDA_TRY(cudaMemcpyAsync(hbuf, misc, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+    PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+    if (hbuf[0] & 1) throw invalid("Data points lie beyond grid. Remove them or increase grid boundaries.");
+    if (hbuf[0] & 2)
+      throw invalid("Data points lie within one rounding of the upper grid bound. Remove them or increase grid boundaries.");
+    if (hbuf[0] & 4) throw invalid("Bootstrap indices must lie in 1:n_samples.");
+    const double cmax = (double)(uint32_t)hbuf[1];
+    double sp = grid->h[0];
+    for (int j = 1; j < N; ++j) sp = sp * grid->h[j];
+    const double denom = (double)n * (sp * sp);
+    const double tmax = (1.0 / ((double)n * sp)) * (1.0 + 1e-12);
+    int ex_m, ex_v;
+    std::frexp((double)nc * std::max(cmax, 1.0) * tmax, &ex_m);
+    std::frexp((double)nc * std::max(cmax, 1.0) * tmax * tmax, &ex_v);
+    const int e_m = 62 - ex_m, e_v = 62 - ex_v;
+    const bool want_sq = sq_out != nullptr && !identity;
+    quantize_kernel<<<nblk, kThreads, 0, st>>>(gd, rh, n, denom, e_m, e_v, qm, want_sq ? qv : nullptr);
+    PKDE_CHECK_LAUNCH();
+    // the sums accumulate as 64-bit integers in the caller's output buffers
+    unsigned long long *am = reinterpret_cast<unsigned long long *>(means_out);
+    unsigned long long *av = want_sq ? reinterpret_cast<unsigned long long *>(sq_out) : nullptr;
+    PKDE_CUDA_TRY(cudaMemsetAsync(am, 0, sizeof(double) * nslots * G, st));
+    if (av) PKDE_CUDA_TRY(cudaMemsetAsync(av, 0, sizeof(double) * nb * G, st));
+    weight_kernel<false><<<noalloc_blocks(sms, nslots * n), kThreads, 0, st>>>(
+        cell, n, nslots, nb, G, N, corner_off, boot_idx, seed, qm, av ? qv : nullptr, am, av, 0, err);
+    PKDE_CHECK_LAUNCH();
+    dequant_kernel<<<noalloc_blocks(sms, nslots * G), kThreads, 0, st>>>(am, nslots * G,
+                                                                                       std::ldexp(1.0, -e_m));
+    PKDE_CHECK_LAUNCH();
+    if (av) {
+      dequant_kernel<<<noalloc_blocks(sms, nb * G), kThreads, 0, st>>>(av, nb * G, std::ldexp(1.0, -e_v));
+      PKDE_CHECK_LAUNCH();
+    }
+    if (sq_out && identity) PKDE_CUDA_TRY(cudaMemsetAsync(sq_out, 0, sizeof(double) * G, st));
     PKDE_CUDA_TRY(cudaStreamSynchronize(st));
   });
 }

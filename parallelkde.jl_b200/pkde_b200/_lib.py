@@ -22,6 +22,7 @@ PKDE_DEVICE_OUTPUT = 2
 EXPORTED = [
     "pkde_create", "pkde_destroy", "pkde_last_error", "pkde_version",
     "pkde_gradepro_default_params", "pkde_gradepro_estimate", "pkde_dirac_sequence",
+    "pkde_dirac_sequence_noalloc",
     "pkde_fft", "pkde_scaled_vmr", "pkde_identify_convergence", "pkde_set_profiling", "pkde_get_stats",
     "pkde_boot_index",
 ]
@@ -77,6 +78,8 @@ def load():
     lib.pkde_gradepro_default_params.argtypes = [ctypes.POINTER(PkdeGradeproParams), i32]
     lib.pkde_gradepro_estimate.argtypes = [vp, ctypes.POINTER(PkdeGradeproParams), vp, i64, vp, u64, vp, vp, u32, vp]
     lib.pkde_dirac_sequence.argtypes = [vp, ctypes.POINTER(PkdeGrid), vp, i64, vp, i32, u64, vp, vp, vp, u32, vp]
+    lib.pkde_dirac_sequence_noalloc.argtypes = [vp, ctypes.POINTER(PkdeGrid), vp, i64, vp, i32, u64, vp, vp, vp,
+                                                vp]
     lib.pkde_fft.argtypes = [vp, i32, vp, vp, i32, i32, u32, vp]
     lib.pkde_scaled_vmr.argtypes = [vp, i64, i32, vp, vp, i32, vp, vp, i64, vp, u32, vp]
     lib.pkde_identify_convergence.argtypes = [vp, i64, vp, vp, vp, vp, vp, dbl, dbl, i64, i64, vp, vp, vp, vp, u32, vp]
