@@ -125,19 +125,31 @@ __device__ void axis_tiles(double2 *smem, const double2 *sm_tw, const double2 *i
   using P = Pow2<LOGN>;
   using I = TileIdx<LOGN, true>;
   const int t = I::bfly();
-  for (int u = 0; u < ntiles; ++u) {
+  auto base_of = [&](int u) {
     const int64_t Lw = (first_tile + u) * P::NL + I::line();
-    const int64_t base = (Lw / inner) * P::N * inner + (Lw % inner);
-    double2 v[8];
+    return (Lw / inner) * P::N * inner + (Lw % inner);
+  };
+  auto load = [&](int64_t base, double2 *x) {
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-      const int k = in_pos<LOGN>(t, r);
-      const double2 x = FROM_SPECTRA ? __ldcs(in + base + (int64_t)k * inner) : __ldcg(in + base + (int64_t)k * inner);
-      v[r] = cscale(x, f[k]);
+      const int64_t off = base + (int64_t)in_pos<LOGN>(t, r) * inner;
+      x[r] = FROM_SPECTRA ? __ldcs(in + off) : __ldcg(in + off);
     }
+  };
+  // the next tile's loads are issued before this tile's FFT, hiding their latency
+  double2 nxt[8];
+  int64_t base = base_of(0);
+  load(base, nxt);
+  for (int u = 0; u < ntiles; ++u) {
+    double2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = cscale(nxt[r], f[in_pos<LOGN>(t, r)]);
+    const int64_t nbase = u + 1 < ntiles ? base_of(u + 1) : base;
+    if (u + 1 < ntiles) load(nbase, nxt);
     tile_fft_reg<LOGN, 1, true>(smem, v, sm_tw);
 #pragma unroll
     for (int i = 0; i < 8; ++i) __stcg(out + base + (int64_t)out_pos<LOGN>(t, i) * inner, v[i]);
+    base = nbase;
   }
 }
 
@@ -456,7 +468,8 @@ void run_engine(pkde_ctx *ctx, const EngineArgs &A, cudaStream_t st) {
   E.P = g->ndim;
   // pairs per group: ring slot (2g arrays) within 16 MB, at least one pair
   const int64_t arr_bytes = (int64_t)sizeof(double2) * E.G;
-  E.g = (int)std::max<int64_t>(1, std::min<int64_t>(E.npairs, (16ll << 20) / (2 * arr_bytes)));
+  const int64_t slot_mb = engine_env_int("PKDE_ENGINE_SLOT_MB", 8, 1, 256);
+  E.g = (int)std::max<int64_t>(1, std::min<int64_t>(E.npairs, (slot_mb << 20) / (2 * arr_bytes)));
   E.J = (E.npairs + E.g - 1) / E.g;
   // pipeline delay between passes of one batch; ring slots cover the delay
   E.D = engine_env_int("PKDE_ENGINE_DELAY", 2, 1, 8);
