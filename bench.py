@@ -164,7 +164,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "batched"])
+    ap.add_argument("--batch", type=int, default=256, help="estimations per batch (--workload batched)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -172,6 +173,8 @@ def main():
                     help="override the workload's bandwidth steps (small profiling runs only)")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
+    if args.workload == "batched":
+        return run_batched(args, world, rank, local, dist)
     x, gspec, kw = workload(args.workload)
     if args.bandwidth_steps:
         kw["n_steps"] = args.bandwidth_steps
@@ -301,6 +304,160 @@ def main():
     if rank == 0 and not args.no_cpu_baseline and world == 1:
         ref = cpu_reference(x, gspec, kw, budget_s=args.cpu_budget)
         line["cpu_baseline"] = {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def batched_jobs(count, seed, device, torch):
+    """The batched workload: `count` independent estimations, dims uniform in {1,2,3},
+    samples log-uniform in [1e3, 1e6] from random 1-4 component Gaussian mixtures, grids
+    256-4096 (1-D), 128^2-512^2 (2-D), 32^3-96^3 (3-D), 100 bandwidth steps, 32
+    bootstraps.  Samples and outputs are device-resident torch tensors; the host copies
+    are kept for the end-to-end leg."""
+    import pkde_b200 as pk
+    from pkde_b200 import workloads as W
+    jobs = []
+    for e, m in enumerate(W.batched_mix(count=count, seed=seed)):
+        grid = pk.find_grid(m["data"], grid_dims=m["dims"])
+        G = int(np.prod(grid.dims))
+        host = np.ascontiguousarray(m["data"].T)
+        jobs.append(dict(grid=grid, host=host, data=torch.from_numpy(host).to(device),
+                         density=torch.empty(G, dtype=torch.float64, device=device),
+                         selected=torch.empty(G, dtype=torch.int32, device=device), seed=e,
+                         n_bootstraps=m["n_bootstraps"], n_steps=m["n_steps"]))
+    return jobs
+
+
+def run_batched(args, world, rank, local, dist):
+    """--workload batched: one step = one pkde_gradepro_estimate_batch call over the whole
+    set.  Also timed once each, on the same set: the plain form (one estimation per call,
+    per-bandwidth-step kernel launches: the structure of the reference's CUDA path) and
+    the step engine one estimation per call."""
+    import torch
+    import pkde_b200 as pk
+    from pkde_b200 import _lib, multi, raw
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pk.load()
+    pk.context(local)
+    jobs = batched_jobs(args.batch, 3 + rank, dev, torch)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    units = sum(int(np.prod(j["grid"].dims)) * (j["n_steps"] + 1) for j in jobs)
+    alg_bytes = sum(16.0 * (j["n_bootstraps"] + 1) * int(np.prod(j["grid"].dims)) * (j["n_steps"] + 1) for j in jobs)
+
+    def batch():
+        raw.gradepro_batch(jobs, device=True, stream=sp, device_id=local)
+
+    for _ in range(args.warmup):
+        batch()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    _lib.get_stats(local, reset=True)
+    _lib.set_profiling(True, local)
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lat = []
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch()
+        b.record(stream)
+        lat.append((a, b))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    _lib.set_profiling(False, local)
+    stats = _lib.get_stats(local, reset=True)
+    t_max = multi.max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
+    lat_ms = sorted(a.elapsed_time(b) for a, b in lat)
+    value = units * args.steps * world / (t_max / 1000.0)
+    est_per_s = len(jobs) * args.steps * world / (t_max / 1000.0)
+    eng_ms = stats["phase_ms"]["step_vmr"] / args.steps
+    achieved = alg_bytes / (eng_ms / 1000.0) / 1e9 if eng_ms > 0 else None
+    peak, peak_kind = peaks()
+
+    # comparators, one pass each over the same set (not part of the timed region)
+    def one_at_a_time():
+        for j in jobs:
+            raw.gradepro_device(j["grid"], j["data"], j["data"].shape[0], j["density"], j["selected"],
+                                seed=j["seed"], stream=sp, device_id=local, n_bootstraps=j["n_bootstraps"],
+                                n_steps=j["n_steps"])
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    engine_single_ms = timed(one_at_a_time)
+    _lib.set_step_path(_lib.PKDE_STEPS_PER_STEP_LAUNCH, local)
+    try:
+        plain_ms = timed(one_at_a_time)
+    finally:
+        _lib.set_step_path(_lib.PKDE_STEPS_AUTO, local)
+    plain_ms = multi.max_over_ranks(plain_ms, dist, dev)
+    engine_single_ms = multi.max_over_ranks(engine_single_ms, dist, dev)
+
+    # e2e: the same batch call with host samples in page-locked memory and host outputs
+    e2e_value = None
+    if not args.no_e2e:
+        pinned = []
+        for j in jobs:
+            t = torch.empty(j["host"].shape, dtype=torch.float64, pin_memory=True)
+            t.numpy()[...] = j["host"]
+            G = int(np.prod(j["grid"].dims))
+            dens = torch.empty(G, dtype=torch.float64, pin_memory=True)
+            sel = torch.empty(G, dtype=torch.int32, pin_memory=True)
+            pinned.append(dict(grid=j["grid"], data=t.numpy(), density=dens.numpy(), selected=sel.numpy(),
+                               seed=j["seed"], n_bootstraps=j["n_bootstraps"], n_steps=j["n_steps"], _keep=(t, dens, sel)))
+        raw.gradepro_batch(pinned, device_id=local)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e0 = time.perf_counter()
+        for _ in range(args.steps):
+            raw.gradepro_batch(pinned, device_id=local)
+        e2e_ms = multi.max_over_ranks((time.perf_counter() - e0) * 1000.0, dist, dev)
+        e2e_value = units * args.steps * world / (e2e_ms / 1000.0)
+    h2d = sum(j["host"].nbytes for j in jobs)
+    d2h = sum(int(np.prod(j["grid"].dims)) * 12 for j in jobs)
+    kinds = {}
+    for j in jobs:
+        d = j["grid"].dims
+        k = f"{len(d)}-D " + ("pow2" if all((v & (v - 1)) == 0 for v in d) else "other")
+        kinds[k] = kinds.get(k, 0) + 1
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"batched: {len(jobs)} estimations per step, dims 1-3, n log-uniform 1e3-1e6, "
+                               "grids 256-4096 / 128^2-512^2 / 32^3-96^3, 101 bandwidths, B=32",
+                   "shapes": kinds, "estimations_per_s": est_per_s,
+                   "plain_form_estimations_per_s": len(jobs) * world / (plain_ms / 1000.0),
+                   "engine_one_at_a_time_estimations_per_s": len(jobs) * world / (engine_single_ms / 1000.0),
+                   "batched_over_plain": (plain_ms / 1000.0) / (t_max / 1000.0 / args.steps),
+                   "p50_ms": lat_ms[len(lat_ms) // 2], "p99_ms": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))],
+                   "l2": "inputs (spectra of all estimations, GBs) larger than the 126 MB L2",
+                   "parallelism": f"independent batches per rank x{world}"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "kernel": "engine_kernel (all N-D estimations of the batch in one launch)",
+                     "peak_source": peak_kind},
+        "phase_ms_per_step": {p: v / args.steps for p, v in stats["phase_ms"].items()},
+        "gpu_launches": stats["launches"],
+        "clocks": clk,
+    }
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -89,6 +89,22 @@ int pkde_gradepro_estimate(pkde_ctx *ctx, const pkde_gradepro_params *p, const d
                            int64_t n, const int32_t *boot_idx, uint64_t seed, double *density_out,
                            int32_t *selected_out, uint32_t flags, void *stream);
 
+/* Several independent estimations in one call (the batched form of
+ * pkde_gradepro_estimate; no counterpart in the reference, whose API estimates one
+ * sample set per call).  Arrays of `count` entries: params[e], data[e] (N_e x n[e]),
+ * boot_idx[e] (or boot_idx == NULL / boot_idx[e] == NULL: seeded draws from seeds[e]),
+ * density_out[e] (G_e FP64), selected_out[e] (G_e int32, or selected_out == NULL /
+ * selected_out[e] == NULL).  Grids, dimensions (1..4), sample and bootstrap counts may
+ * all differ.  Every phase runs for all estimations before the next (one host read-back
+ * per phase for the whole call) and the bandwidth steps of all N-D power-of-two
+ * estimations share one persistent launch.  Each estimation's results are identical to
+ * what pkde_gradepro_estimate gives for it alone.  An invalid estimation fails the call
+ * (the message names its index). */
+int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradepro_params *params,
+                                 const double *const *data, const int64_t *n, const int32_t *const *boot_idx,
+                                 const uint64_t *seeds, double *const *density_out, int32_t *const *selected_out,
+                                 uint32_t flags, void *stream);
+
 /* Dirac-sequence binning of bootstrap resamples onto the grid.
  * Replaces initialize_dirac_sequence(Val(:cuda), ...) (DirectSpace.jl:289-362) and its
  * kernel generate_dirac_cuda! (:364-477), following the CPU arithmetic (:196-287).
@@ -137,6 +153,23 @@ int pkde_identify_convergence(pkde_ctx *ctx, int64_t G, double *density, const d
                               int64_t steps_over, double *minima, uint16_t *counters_low,
                               uint16_t *counters_over, uint8_t *low_density_flags, uint32_t flags,
                               void *stream);
+
+/* How the bandwidth steps of an estimation are executed (a context setting).
+ *   PKDE_STEPS_AUTO          : the persistent step engine for N-D grids with axes of
+ *                              2..2048 points, one CTA per bandwidth step for 1-D
+ *                              power-of-two grids of 256..4096 points, else per-step
+ *                              kernel launches;
+ *   PKDE_STEPS_PER_STEP_LAUNCH: every estimation on the plain form -- per bandwidth step
+ *                              and pair group, one kernel launch per FFT axis, then the
+ *                              VMR and the means/convergence launches, estimations one
+ *                              after another.  This mirrors the reference's CUDA path
+ *                              (GradeProEstimator.jl:968-1051: propagate, ifft, VMR,
+ *                              means, convergence per step) and is the comparator of the
+ *                              batched form; results agree with AUTO to FP64 round-off.
+ * No counterpart in the reference. */
+#define PKDE_STEPS_AUTO 0
+#define PKDE_STEPS_PER_STEP_LAUNCH 1
+int pkde_set_step_path(pkde_ctx *ctx, int path);
 
 /* Launch accounting and per-phase device time, for tracing and the roofline report.
  * No counterpart in the reference, which has no tracing.

@@ -330,10 +330,127 @@ static DiracScales dirac_core(pkde_ctx *ctx, const pkde_grid *g, const double *d
   return DiracScales{sm, sv};
 }
 
-// Estimator entry: paired spectra-ready layout (nboot resamples + identity).
-void dirac_paired(pkde_ctx *ctx, const pkde_grid *g, const double *d_data, int64_t n, const int32_t *d_idx,
-                  int64_t nboot, uint64_t seed, double2 *spectra, cudaStream_t st) {
-  dirac_core(ctx, g, d_data, n, d_idx, nboot, true, seed, true, spectra, nullptr, nullptr, nullptr, st);
+// Estimator entry: paired spectra-ready layout (nboot resamples + identity), in two
+// phases around one host read-back of the error flags and the largest count, so that
+// the estimations of a batch share one synchronisation.
+size_t dirac_job_scratch(const pkde_grid *g, int64_t n, int64_t nboot) {
+  const int N = g->ndim;
+  const int64_t nc = int64_t(1) << N;
+  const int64_t G = grid_size(g);
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  return al(sizeof(uint32_t) * n) + al(sizeof(double) * N * n + sizeof(unsigned long long) * 2 * nc * n) +
+         al(sizeof(uint32_t) * (nboot + 1) * G);
+}
+
+void dirac_job_bind(DiracJob &j, char *scratch, int *misc) {
+  const int N = j.g->ndim;
+  const int64_t nc = int64_t(1) << N;
+  const int64_t G = grid_size(j.g);
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  j.cell = (uint32_t *)scratch;
+  scratch += al(sizeof(uint32_t) * j.n);
+  j.rh = (double *)scratch;
+  scratch += al(sizeof(double) * N * j.n + sizeof(unsigned long long) * 2 * nc * j.n);
+  j.counts = (uint32_t *)scratch;
+  (void)G;
+  j.misc = misc;
+}
+
+// Phase A: bounds check and cell pre-pass, exact counts, largest count (misc[0] error
+// bits, misc[1] max count).  Nothing is read back here.
+void dirac_job_phase_a(pkde_ctx *ctx, DiracJob &j, cudaStream_t st) {
+  const pkde_grid *g = j.g;
+  grid_validate(g);
+  const int64_t n = j.n;
+  if (n < 1 || n >= (int64_t(1) << 31)) throw invalid("number of samples must be in [1, 2^31)");
+  GridDev gd = to_dev(g);
+  const int64_t G = grid_size(g);
+  const int N = g->ndim;
+  const int nc = 1 << N;
+  const int64_t nslots = j.nboot + 1;
+  int *misc = j.misc;
+  unsigned int *maxc = reinterpret_cast<unsigned int *>(misc + 1);
+  int64_t *corner_off = reinterpret_cast<int64_t *>(misc + 8);  // 16 entries
+  for (int c = 0; c < nc; ++c) {
+    int64_t o = 0;
+    for (int q = 0; q < N; ++q)
+      if (!((c >> (N - 1 - q)) & 1)) o += gd.stride[q];
+    j.corner_off_h[c] = o;
+  }
+  PKDE_CUDA_TRY(cudaMemsetAsync(misc, 0, 64, st));
+  PKDE_CUDA_TRY(cudaMemcpyAsync(corner_off, j.corner_off_h, sizeof(int64_t) * nc, cudaMemcpyHostToDevice, st));
+  PKDE_CUDA_TRY(cudaMemsetAsync(j.counts, 0, sizeof(uint32_t) * nslots * G, st));
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    prepass_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(gd, j.d_data, n, j.cell, j.rh,
+                                                                                    misc);
+  }
+  PKDE_CHECK_LAUNCH();
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    count_kernel<<<grid_blocks(ctx, nslots * n), kThreads, 0, st>>>(j.cell, n, nslots, j.nboot, G, j.d_idx, j.seed,
+                                                                    j.counts, misc);
+  }
+  PKDE_CHECK_LAUNCH();
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    max_kernel<<<grid_blocks(ctx, nslots * G), kThreads, 0, st>>>(j.counts, nslots * G, maxc);
+  }
+  PKDE_CHECK_LAUNCH();
+}
+
+// Phase B, given misc[0..1] read back: error check, fixed-point scales, quantised
+// corner terms, scatter into the paired spectra slots, conversion to FP64.
+void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_t st) {
+  const pkde_grid *g = j.g;
+  if (hmisc[0] & 1) throw invalid("Data points lie beyond grid. Remove them or increase grid boundaries.");
+  if (hmisc[0] & 2)
+    throw invalid("Data points lie within one rounding of the upper grid bound. Remove them or increase grid boundaries.");
+  if (hmisc[0] & 4) throw invalid("Bootstrap indices must lie in 1:n_samples.");
+  const double cmax = (double)(uint32_t)hmisc[1];
+  GridDev gd = to_dev(g);
+  const int64_t G = grid_size(g);
+  const int N = g->ndim;
+  const int nc = 1 << N;
+  const int64_t n = j.n;
+  const int64_t nboot = j.nboot;
+  const int64_t nslots = nboot + 1;
+  unsigned long long *qm = reinterpret_cast<unsigned long long *>(j.rh + N * n);
+  unsigned long long *qv = qm + (int64_t)nc * n;
+  const int64_t *corner_off = reinterpret_cast<const int64_t *>(j.misc + 8);
+  // term <= prod(h) / (n prod(h)^2); a cell sums at most 2^N * cmax terms.
+  double sp = g->h[0];
+  for (int q = 1; q < N; ++q) sp = sp * g->h[q];
+  const double denom = (double)n * (sp * sp);
+  const double tmax = (1.0 / ((double)n * sp)) * (1.0 + 1e-12);
+  const double bound_m = (double)nc * std::max(cmax, 1.0) * tmax;
+  const double bound_v = (double)nc * std::max(cmax, 1.0) * tmax * tmax;
+  int ex_m, ex_v;
+  std::frexp(bound_m, &ex_m);  // bound_m < 2^ex_m
+  std::frexp(bound_v, &ex_v);
+  const int e_m = 62 - ex_m;
+  const int e_v = 62 - ex_v;
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    quantize_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(gd, j.rh, n, denom, e_m, e_v, qm,
+                                                                                     qv);
+  }
+  PKDE_CHECK_LAUNCH();
+  const double sm = std::ldexp(1.0, -e_m), sv = std::ldexp(1.0, -e_v);
+  const int64_t npairs = (nboot + 1) / 2;
+  unsigned long long *acc = reinterpret_cast<unsigned long long *>(j.paired_out);
+  PKDE_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double2) * (2 * npairs + 1) * G, st));
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    weight_kernel<true><<<grid_blocks(ctx, nslots * n), kThreads, 0, st>>>(
+        j.cell, n, nslots, nboot, G, N, corner_off, j.d_idx, j.seed, qm, qv, acc, nullptr, npairs, j.misc);
+  }
+  PKDE_CHECK_LAUNCH();
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    dequant_paired_kernel<<<grid_blocks(ctx, (2 * npairs + 1) * G * 2), kThreads, 0, st>>>(acc, G, npairs, sm, sv);
+  }
+  PKDE_CHECK_LAUNCH();
 }
 
 }  // namespace pkde

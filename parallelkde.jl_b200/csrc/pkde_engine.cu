@@ -25,6 +25,9 @@
 // CTA and read by another is loaded with ld.global.cg (L2), never through L1.
 #include <cuda/atomic>
 
+#include <algorithm>
+#include <cstring>
+
 #include "pkde_regfft.cuh"
 #include "pkde_step.cuh"
 
@@ -35,6 +38,7 @@ namespace {
 constexpr int kEngineThreads = 256;
 constexpr long long kSpinLimit = 20000000;  // ~1-2 s of polling, then the run aborts
 
+// One estimation's part of a launch (device-resident descriptor).
 struct EngineEst {
   int ndim;
   int logn[4];
@@ -52,17 +56,35 @@ struct EngineEst {
   double invG, inv_n, eps;
   int64_t steps_low, steps_over;
   StepState cs;
-  int64_t NB;            // batches
-  int64_t nrounds;
-  const int64_t *round_start;  // nrounds + 1 prefix sums of items per round
-  int *cnt;              // NB x P completed tiles per (batch, pass)
-  int *fin;              // NB x Tf per-tile final-pass done flags
-  int Tf;                // final-pass tiles per batch
-  int tpi[4];            // axis passes: tiles per work item, by axis
-  int D;                 // pass p of batch b runs in round b + p*D
-  int *next;             // work counter
-  int *error;            // 1: dependency wait timed out
-  const double2 *tw[13]; // per-stage twiddle tables by log2(line length)
+  int64_t NB;                  // batches
+  int64_t nrounds;             // local rounds
+  const int64_t *round_start;  // nrounds + 1 prefix sums of items per local round
+  int *cnt;                    // NB x P completed tiles per (batch, pass)
+  int *fin;                    // NB x Tf per-tile final-pass done flags
+  int Tf;                      // final-pass tiles per batch
+  int tpi[4];                  // axis passes: tiles per work item, by axis
+  int D;                       // pass p of batch b runs in local round b + p*D
+  int tl[4];                   // lines per tile, by axis
+  int gen[4];                  // 1: the axis uses the shared-memory mixed-radix FFT (any length)
+  const double2 *twg[4];       // generic axes: twiddle table (cos, sin)(2 pi m / n), m < n
+  FftPlan plan[4];             // generic axes: Stockham radix sequence
+};
+
+// A launch over one or more estimations.  Estimation e runs its local round r in global
+// round start_e + r; the global item order is round-major, and within a global round
+// estimation-major.  Segment k covers items [seg_start[k], seg_start[k+1]) = the items
+// of local round seg[k].y of estimation seg[k].x.  Every dependency of an item is an
+// item of the same estimation in an earlier local round, hence earlier in this order.
+struct EngineRun {
+  const EngineEst *est;
+  int count;
+  const int64_t *seg_start;  // nseg + 1
+  const int2 *seg;           // nseg
+  int64_t nseg;
+  int64_t total_items;
+  int *next;   // work counter
+  int *error;  // 1: dependency wait timed out
+  const double2 *tw[13];  // per-stage twiddle tables by log2(line length)
 };
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
@@ -75,11 +97,11 @@ __device__ __forceinline__ void add_release(int *p, int v) {
 }
 
 // Spin until *p >= target (thread 0 only).  Returns false on timeout or abort.
-__device__ bool wait_geq(const EngineEst &E, const int *p, int target) {
+__device__ bool wait_geq(int *error, const int *p, int target) {
   long long it = 0;
   while (ld_acquire(p) < target) {
-    if (++it > kSpinLimit || ld_acquire(E.error)) {
-      atomicExch(E.error, 1);
+    if (++it > kSpinLimit || ld_acquire(error)) {
+      atomicExch(error, 1);
       return false;
     }
     __nanosleep(64);
@@ -99,7 +121,7 @@ __host__ __device__ __forceinline__ int batch_arrays(const EngineEst &E, int64_t
 __host__ __device__ __forceinline__ int pass_tiles(const EngineEst &E, int64_t b, int p) {
   if (p == E.P - 1) return E.Tf;
   const int a = E.ndim - 1 - p;
-  return (int)(batch_arrays(E, b) * (E.G / E.dims[a]) / ((int64_t)tile_lines_of(E.logn[a]) * E.tpi[a]));
+  return (int)(batch_arrays(E, b) * (E.G / E.dims[a]) / ((int64_t)E.tl[a] * E.tpi[a]));
 }
 
 // ------------------------------------------------------------------ tile bodies
@@ -249,32 +271,125 @@ __device__ void means_tile(double2 *smem, double2 *sm_tw, const double2 *in, con
   }
 }
 
-// ------------------------------------------------------------------ the engine
-struct Decoded {
-  int64_t b;
-  int p;
-  int64_t tile;
-};
+// ------------------------------------------------- tile bodies, any line length
+// The same three tile kinds for axes whose length is not a power of two in 16..2048:
+// TL lines staged in shared memory (two buffers of TL x (n + 1)), the Stockham
+// mixed-radix FFT of pkde_internal.cuh (radix 8/4/2/3/5, generic odd radix), twiddles
+// from the table of the line length.
 
-__device__ bool decode(const EngineEst &E, int64_t item, int64_t &round, Decoded &d) {
-  while (round < E.nrounds && E.round_start[round + 1] <= item) ++round;
-  if (round >= E.nrounds) return false;
-  int64_t off = item - E.round_start[round];
-  for (int p = E.P - 1; p >= 0; --p) {
-    const int64_t b = round - (int64_t)p * E.D;
-    if (b < 0 || b >= E.NB) continue;
-    const int n = pass_tiles(E, b, p);
-    if (off < n) {
-      d.b = b;
-      d.p = p;
-      d.tile = off;
-      return true;
+// Lines L0 .. L0+TL-1 along an axis with stride `inner`; element k of line L sits at
+// (L / inner) * n * inner + (L % inner) + k * inner.  Consecutive threads take
+// consecutive lines (coalesced wherever adjacent lines are adjacent in memory).
+template <bool FROM_SPECTRA>
+__device__ void axis_tiles_gen(double2 *smem, const double2 *in, double2 *out, int n, int64_t inner,
+                               int64_t first_tile, int ntiles, const double *f, int TL, const FftPlan &plan,
+                               const double2 *tw) {
+  const int pitch = n + 1;
+  double2 *bufA = smem, *bufB = smem + TL * pitch;
+  const int npts = TL * n;
+  for (int u = 0; u < ntiles; ++u) {
+    const int64_t L0 = (first_tile + u) * TL;
+    for (int e = threadIdx.x; e < npts; e += blockDim.x) {
+      const int k = e / TL, l = e - k * TL;
+      const int64_t L = L0 + l;
+      const int64_t off = (L / inner) * n * inner + (L % inner) + (int64_t)k * inner;
+      const double2 x = FROM_SPECTRA ? __ldcs(in + off) : __ldcg(in + off);
+      bufA[l * pitch + k] = cscale(x, f[k]);
     }
-    off -= n;
+    __syncthreads();
+    const double2 *res = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
+    for (int e = threadIdx.x; e < npts; e += blockDim.x) {
+      const int k = e / TL, l = e - k * TL;
+      const int64_t L = L0 + l;
+      const int64_t off = (L / inner) * n * inner + (L % inner) + (int64_t)k * inner;
+      __stcg(out + off, res[l * pitch + k]);
+    }
+    __syncthreads();
   }
-  return false;
 }
 
+// Final pass, TL contiguous rows of length n1 (npts = TL * n1 <= 8 * kEngineThreads):
+// inverse FFT of the z and w rows of every pair, VMR of both bootstraps of a pair and
+// the Welford update over bootstraps in order (state per point in shared memory).
+__device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, int npairs, int b0, int nboot,
+                             const double *fz, const double *fw, double cz, double cw, double inv_n, int64_t G,
+                             double *wst, int first, int64_t tile, int n1, int TL, const FftPlan &plan,
+                             const double2 *tw) {
+  const int pitch = n1 + 1;
+  double2 *bufA = smem, *bufB = smem + TL * pitch;
+  const int npts = TL * n1;
+  const int64_t rbase = tile * npts;
+  for (int e = threadIdx.x; e < npts; e += blockDim.x)
+    state[e] = first ? make_double2(0.0, 0.0) : make_double2(__ldcg(wst + rbase + e), __ldcg(wst + G + rbase + e));
+  for (int p = 0; p < npairs; ++p) {
+    const double2 *zs = in + (int64_t)(2 * p) * G + rbase;
+    const double2 *ws = zs + G;
+    double2 zval[8];
+    for (int e = threadIdx.x; e < npts; e += blockDim.x) {
+      const int l = e / n1, k = e - l * n1;
+      bufA[l * pitch + k] = cscale(__ldcg(zs + e), cz * fz[k]);
+    }
+    __syncthreads();
+    const double2 *rz = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = threadIdx.x + q * kEngineThreads;
+      if (e < npts) zval[q] = rz[(e / n1) * pitch + (e % n1)];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < npts; e += blockDim.x) {
+      const int l = e / n1, k = e - l * n1;
+      bufA[l * pitch + k] = cscale(__ldcg(ws + e), cw * fw[k]);
+    }
+    __syncthreads();
+    const double2 *rw = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
+    const int b = b0 + 2 * p;
+    const double inv_a = 1.0 / (double)(b + 1), inv_b = 1.0 / (double)(b + 2);
+    const bool has_b = b + 1 < nboot;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = threadIdx.x + q * kEngineThreads;
+      if (e < npts) {
+        const double2 w = rw[(e / n1) * pitch + (e % n1)];
+        double2 st = state[e];
+        welford(vmr_of(zval[q].x, w.x, inv_n), inv_a, st.x, st.y);
+        if (has_b) welford(vmr_of(zval[q].y, w.y, inv_n), inv_b, st.x, st.y);
+        state[e] = st;
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < npts; e += blockDim.x) {
+    const double2 st = state[e];
+    __stcg(wst + rbase + e, st.x);
+    __stcg(wst + G + rbase + e, st.y);
+  }
+}
+
+__device__ void means_tile_gen(double2 *smem, const double2 *in, const double *fz, double cz, const double *wst,
+                               int64_t G, int nboot, double vscale, double dlogt, double eps, int64_t steps_low,
+                               int64_t steps_over, const StepState &cs, int step, int64_t tile, int n1, int TL,
+                               const FftPlan &plan, const double2 *tw) {
+  const int pitch = n1 + 1;
+  double2 *bufA = smem, *bufB = smem + TL * pitch;
+  const int npts = TL * n1;
+  const int64_t rbase = tile * npts;
+  for (int e = threadIdx.x; e < npts; e += blockDim.x) {
+    const int l = e / n1, k = e - l * n1;
+    bufA[l * pitch + k] = cscale(__ldcg(in + rbase + e), cz * fz[k]);
+  }
+  __syncthreads();
+  const double2 *res = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
+  for (int e = threadIdx.x; e < npts; e += blockDim.x) {
+    const double2 z = res[(e / n1) * pitch + (e % n1)];
+    const int64_t gi = rbase + e;
+    const double mu = sqrt(z.x * z.x + z.y * z.y);
+    const double m2 = __ldcg(wst + G + gi);
+    step_update<true>(cs, gi, mu, vscale * m2 / (double)(nboot - 1), dlogt, eps, steps_low, steps_over, step);
+  }
+}
+
+// ------------------------------------------------------------------ the engine
 #define PKDE_ENGINE_SWITCH(LN, CALL) \
   switch (LN) {                      \
     case 4: CALL(4); break;          \
@@ -288,54 +403,105 @@ __device__ bool decode(const EngineEst &E, int64_t item, int64_t &round, Decoded
     default: break;                  \
   }
 
-__global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineEst E, int64_t total_items, int max_tile,
-                                                                   int max_tw) {
+// GEN: some estimation of the launch has an axis on the shared-memory FFT path (a
+// separate instantiation keeps the register pressure of all-power-of-two launches low).
+template <bool GEN>
+__global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineRun R, int max_tile) {
   extern __shared__ double2 smem[];
   double2 *tile_mem = smem;
   double2 *state = smem + max_tile;
   double2 *sm_tw = state + 8 * kEngineThreads;
-  __shared__ int64_t s_next;
-  __shared__ int s_ok;
+  __shared__ EngineEst sE;  // descriptor of the estimation the current item belongs to
+  __shared__ int64_t s_next, s_b, s_tile, s_round, s_off;
+  __shared__ int s_p, s_ok, s_e;
   int cached_tw = -1;
-  int64_t round = 0;
-  (void)max_tw;
+  int cached_e = -1;
+  int64_t cur = 0;  // segment cursor (warp 0; items of a CTA increase, so it only moves forward)
   // The next item is taken while the current one runs (items are taken in increasing
   // order per CTA, so every wait still points to an earlier item).
-  if (threadIdx.x == 0) s_next = (int64_t)atomicAdd(E.next, 1);
+  if (threadIdx.x == 0) s_next = (int64_t)atomicAdd(R.next, 1);
   __syncthreads();
   int64_t item = s_next;
   for (;;) {
-    if (item >= total_items) break;
-    __syncthreads();  // everyone has read s_next
-    if (threadIdx.x == 0) s_next = ld_acquire(E.error) ? total_items : (int64_t)atomicAdd(E.next, 1);
-    Decoded d;
-    if (!decode(E, item, round, d)) break;
-    const int64_t b = d.b;
-    const int p = d.p;
-    const int64_t s = b / (E.J + 1);
-    const int j = (int)(b % (E.J + 1));
-    const bool means = j == E.J;
-    const int64_t slot = b % E.Q;
-    double2 *slot_base = E.slots + slot * E.slot_elems;
-    // ---- dependencies (thread 0 spins; acquire orders the data reads after it)
-    if (threadIdx.x == 0) {
-      bool ok = true;
-      if (p == 0) {
-        if (b >= E.Q) ok = wait_geq(E, E.cnt + (b - E.Q) * E.P + (E.P - 1), pass_tiles(E, b - E.Q, E.P - 1));
-      } else {
-        ok = wait_geq(E, E.cnt + b * E.P + (p - 1), pass_tiles(E, b, p - 1));
+    if (item >= R.total_items) break;
+    __syncthreads();  // everyone has read s_next and finished with sE
+    if (threadIdx.x == 0) s_next = ld_acquire(R.error) ? R.total_items : (int64_t)atomicAdd(R.next, 1);
+    // ---- segment of `item`: seg_start is increasing, so the lanes whose entry is
+    // <= item form a prefix; advance by its length (32 entries per iteration)
+    if (threadIdx.x < 32) {
+      for (;;) {
+        const int64_t k = cur + 1 + threadIdx.x;
+        const bool le = k <= R.nseg && __ldg(R.seg_start + k) <= item;
+        const int c = __popc(__ballot_sync(0xffffffffu, le));
+        cur += c;
+        if (c < 32) break;
       }
-      if (ok && p == E.P - 1) {
-        if (j > 0) ok = wait_geq(E, E.fin + (b - 1) * E.Tf + d.tile, 1);  // Welford order / all groups done
-        if (ok && j == 0 && s >= 2)                                         // state slot free
-          ok = wait_geq(E, E.fin + ((s - 2) * (E.J + 1) + E.J) * E.Tf + d.tile, 1);
-        if (ok && means && s >= 1)                                          // convergence order
-          ok = wait_geq(E, E.fin + ((s - 1) * (E.J + 1) + E.J) * E.Tf + d.tile, 1);
+      if (threadIdx.x == 0) {
+        const int2 sg = __ldg(R.seg + cur);
+        s_e = sg.x;
+        s_round = sg.y;
+        s_off = item - __ldg(R.seg_start + cur);
+      }
+    }
+    __syncthreads();
+    if (s_e != cached_e) {
+      cached_e = s_e;
+      const int *src = reinterpret_cast<const int *>(R.est + cached_e);
+      int *dst = reinterpret_cast<int *>(&sE);
+      for (int i = threadIdx.x; i < (int)(sizeof(EngineEst) / sizeof(int)); i += blockDim.x) dst[i] = __ldg(src + i);
+      __syncthreads();
+    }
+    const EngineEst &E = sE;
+    // ---- decode (thread 0) and dependencies (thread 0 spins; acquire orders the data
+    // reads after it)
+    if (threadIdx.x == 0) {
+      bool ok = false;
+      int64_t off = s_off;
+      for (int p = E.P - 1; p >= 0; --p) {
+        const int64_t b = s_round - (int64_t)p * E.D;
+        if (b < 0 || b >= E.NB) continue;
+        const int n = pass_tiles(E, b, p);
+        if (off < n) {
+          s_b = b;
+          s_p = p;
+          s_tile = off;
+          ok = true;
+          break;
+        }
+        off -= n;
+      }
+      if (ok) {
+        const int64_t b = s_b;
+        const int p = s_p;
+        const int64_t s = b / (E.J + 1);
+        const int j = (int)(b % (E.J + 1));
+        if (p == 0) {
+          if (b >= E.Q) ok = wait_geq(R.error, E.cnt + (b - E.Q) * E.P + (E.P - 1), pass_tiles(E, b - E.Q, E.P - 1));
+        } else {
+          ok = wait_geq(R.error, E.cnt + b * E.P + (p - 1), pass_tiles(E, b, p - 1));
+        }
+        if (ok && p == E.P - 1) {
+          if (j > 0) ok = wait_geq(R.error, E.fin + (b - 1) * E.Tf + s_tile, 1);  // Welford order / all groups done
+          if (ok && j == 0 && s >= 2)                                                // state slot free
+            ok = wait_geq(R.error, E.fin + ((s - 2) * (E.J + 1) + E.J) * E.Tf + s_tile, 1);
+          if (ok && j == E.J && s >= 1)                                              // convergence order
+            ok = wait_geq(R.error, E.fin + ((s - 1) * (E.J + 1) + E.J) * E.Tf + s_tile, 1);
+        }
+      } else {
+        atomicExch(R.error, 1);  // the schedule and the descriptor disagree
       }
       s_ok = ok;
     }
     __syncthreads();
     if (!s_ok) break;
+    const int64_t b = s_b;
+    const int p = s_p;
+    const int64_t tile = s_tile;
+    const int64_t s = b / (E.J + 1);
+    const int j = (int)(b % (E.J + 1));
+    const bool means = j == E.J;
+    const int64_t slot = b % E.Q;
+    double2 *slot_base = E.slots + slot * E.slot_elems;
     // ---- work
     const double *fzs = E.fz + s * E.tab_stride;
     const double *fws = E.fw + s * E.tab_stride;
@@ -344,9 +510,9 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineEst E, 
       const int ln = E.logn[a];
       const int64_t lines = E.G / E.dims[a];
       const int tpi = E.tpi[a];
-      const int64_t ipa = lines / ((int64_t)tile_lines_of(ln) * tpi);  // items per array
-      const int64_t arr = d.tile / ipa;
-      const int64_t first_tile = (d.tile % ipa) * tpi;
+      const int64_t ipa = lines / ((int64_t)E.tl[a] * tpi);  // items per array
+      const int64_t arr = tile / ipa;
+      const int64_t first_tile = (tile % ipa) * tpi;
       int64_t inner = 1;
       for (int q = 0; q < a; ++q) inner *= E.dims[q];
       const double2 *in = p == 0 ? (means ? E.spectra + (int64_t)(2 * E.npairs) * E.G
@@ -357,13 +523,22 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineEst E, 
       const double *f = (!means && (arr & 1)) ? fws + E.aoff[a] : fzs + E.aoff[a];
 #define PKDE_AXIS(L)                                                                      \
   {                                                                                       \
-    stage_tw<L>(sm_tw, E.tw[L], cached_tw, L);                                            \
+    stage_tw<L>(sm_tw, R.tw[L], cached_tw, L);                                            \
     if (p == 0)                                                                           \
       axis_tiles<L, true>(tile_mem, sm_tw, in, out, inner, first_tile, tpi, f);           \
     else                                                                                  \
       axis_tiles<L, false>(tile_mem, sm_tw, in, out, inner, first_tile, tpi, f);          \
   }
-      PKDE_ENGINE_SWITCH(ln, PKDE_AXIS)
+      if (GEN && E.gen[a]) {
+        if (p == 0)
+          axis_tiles_gen<true>(tile_mem, in, out, (int)E.dims[a], inner, first_tile, tpi, f, E.tl[a], E.plan[a],
+                               E.twg[a]);
+        else
+          axis_tiles_gen<false>(tile_mem, in, out, (int)E.dims[a], inner, first_tile, tpi, f, E.tl[a], E.plan[a],
+                                E.twg[a]);
+      } else {
+        PKDE_ENGINE_SWITCH(ln, PKDE_AXIS)
+      }
 #undef PKDE_AXIS
     } else {
       const int ln = E.logn[0];
@@ -371,21 +546,33 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineEst E, 
         const int np = batch_arrays(E, b) / 2;
 #define PKDE_VMR(L)                                                                                         \
   {                                                                                                         \
-    stage_tw<L>(sm_tw, E.tw[L], cached_tw, L);                                                              \
+    stage_tw<L>(sm_tw, R.tw[L], cached_tw, L);                                                              \
     vmr_tile<L>(tile_mem, state, sm_tw, slot_base, np, 2 * j * E.g, E.nboot, fzs + E.aoff[0],               \
                 fws + E.aoff[0], E.invG, E.invG * E.cw[s], E.inv_n, E.G, E.wstate + (s & 1) * 2 * E.G,      \
-                j == 0, d.tile);                                                                            \
+                j == 0, tile);                                                                              \
   }
-        PKDE_ENGINE_SWITCH(ln, PKDE_VMR)
+        if (GEN && E.gen[0]) {
+          vmr_tile_gen(tile_mem, state, slot_base, np, 2 * j * E.g, E.nboot, fzs + E.aoff[0], fws + E.aoff[0], E.invG,
+                       E.invG * E.cw[s], E.inv_n, E.G, E.wstate + (s & 1) * 2 * E.G, j == 0, tile, (int)E.dims[0],
+                       E.tl[0], E.plan[0], E.twg[0]);
+        } else {
+          PKDE_ENGINE_SWITCH(ln, PKDE_VMR)
+        }
 #undef PKDE_VMR
       } else {
 #define PKDE_MEANS(L)                                                                                        \
   {                                                                                                          \
-    stage_tw<L>(sm_tw, E.tw[L], cached_tw, L);                                                               \
+    stage_tw<L>(sm_tw, R.tw[L], cached_tw, L);                                                               \
     means_tile<L>(tile_mem, sm_tw, slot_base, fzs + E.aoff[0], E.invG, E.wstate + (s & 1) * 2 * E.G, E.G,     \
-                  E.nboot, E.vscale[s], E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs, (int)s, d.tile); \
+                  E.nboot, E.vscale[s], E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs, (int)s, tile);   \
   }
-        PKDE_ENGINE_SWITCH(ln, PKDE_MEANS)
+        if (GEN && E.gen[0]) {
+          means_tile_gen(tile_mem, slot_base, fzs + E.aoff[0], E.invG, E.wstate + (s & 1) * 2 * E.G, E.G, E.nboot,
+                         E.vscale[s], E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs, (int)s, tile,
+                         (int)E.dims[0], E.tl[0], E.plan[0], E.twg[0]);
+        } else {
+          PKDE_ENGINE_SWITCH(ln, PKDE_MEANS)
+        }
 #undef PKDE_MEANS
       }
     }
@@ -393,7 +580,7 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineEst E, 
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
-      if (p == E.P - 1) add_release(E.fin + b * E.Tf + d.tile, 1);
+      if (p == E.P - 1) add_release(E.fin + b * E.Tf + tile, 1);
       add_release(E.cnt + b * E.P + p, 1);
     }
     item = s_next;
@@ -437,49 +624,80 @@ int engine_env_int(const char *name, int dflt, int lo, int hi) {
   return x < lo ? lo : (x > hi ? hi : x);
 }
 
-bool engine_ok(const pkde_grid *g) {
-  if (g->ndim < 2) return false;
+// Tile shape of grid axis j: the register radix-8 FFT where the axis is a power of two
+// in 16..2048 whose tiles line up with the layout; otherwise the shared-memory
+// mixed-radix FFT for lengths up to 2048, TL lines per tile (a power of two dividing
+// the number of lines, TL x n <= 2048).
+struct AxisShape {
+  bool ok;
+  int gen;
+  int tl;
+};
+static AxisShape axis_shape(const pkde_grid *g, int j) {
   const int64_t G = grid_size(g);
   int64_t inner = 1;
-  for (int j = 0; j < g->ndim; ++j) {
-    const int ln = ilog2_pow2(g->dims[j]);
-    if (ln < 4 || ln > 11) return false;
+  for (int q = 0; q < j; ++q) inner *= g->dims[q];
+  const int64_t n = g->dims[j];
+  const int64_t lines = G / n;
+  const int ln = ilog2_pow2(n);
+  if (ln >= 4 && ln <= 11) {
     const int nl = tile_lines_of(ln);
-    if ((G / g->dims[j]) % nl) return false;
-    if (j > 0 && inner % nl) return false;
-    inner *= g->dims[j];
+    if (lines % nl == 0 && (j == 0 || inner % nl == 0)) return AxisShape{true, 0, nl};
   }
+  if (n < 2 || n > 2048) return AxisShape{false, 0, 0};
+  int tl = 1;
+  const int64_t cap = std::min<int64_t>(16, 2048 / n);
+  while (tl * 2 <= cap && lines % (tl * 2) == 0) tl *= 2;
+  return AxisShape{true, 1, tl};
+}
+
+bool engine_ok(const pkde_grid *g) {
+  if (g->ndim < 2) return false;
+  for (int j = 0; j < g->ndim; ++j)
+    if (!axis_shape(g, j).ok) return false;
   return true;
 }
 
-void run_engine(pkde_ctx *ctx, const EngineArgs &A, cudaStream_t st) {
+namespace {
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Host-side descriptor of one estimation (device pointers filled in later).
+EngineEst describe(const EngineArgs &A) {
   const pkde_grid *g = A.grid;
   EngineEst E{};
   E.ndim = g->ndim;
   E.G = grid_size(g);
   for (int j = 0; j < g->ndim; ++j) {
+    const AxisShape sh = axis_shape(g, j);
     E.dims[j] = g->dims[j];
-    E.logn[j] = ilog2_pow2(g->dims[j]);
+    E.gen[j] = sh.gen;
+    E.tl[j] = sh.tl;
+    E.logn[j] = sh.gen ? -1 : ilog2_pow2(g->dims[j]);
     E.aoff[j] = A.aoff[j];
   }
   E.npairs = A.npairs;
   E.nboot = A.nboot;
   E.S = A.S;
   E.P = g->ndim;
-  // pairs per group: ring slot (2g arrays) within 16 MB, at least one pair
+  // pairs per group: ring slot (2g arrays) within 32 MB, at least one pair.  Larger
+  // groups mean fewer, wider batches (more independent tiles per round); measured on
+  // 512 x 512 / B = 64: 74 ms at 8 MB, 58.6 ms at 16 MB, 56.9 ms at 32 MB.
   const int64_t arr_bytes = (int64_t)sizeof(double2) * E.G;
-  const int64_t slot_mb = engine_env_int("PKDE_ENGINE_SLOT_MB", 8, 1, 256);
+  const int64_t slot_mb = engine_env_int("PKDE_ENGINE_SLOT_MB", 32, 1, 256);
   E.g = (int)std::max<int64_t>(1, std::min<int64_t>(E.npairs, (slot_mb << 20) / (2 * arr_bytes)));
   E.J = (E.npairs + E.g - 1) / E.g;
   // pipeline delay between passes of one batch; ring slots cover the delay
   E.D = engine_env_int("PKDE_ENGINE_DELAY", 2, 1, 8);
   E.Q = (E.P - 1) * E.D + 2;
   E.NB = (int64_t)E.S * (E.J + 1);
-  E.Tf = (int)((E.G / E.dims[0]) / tile_lines_of(E.logn[0]));
+  E.Tf = (int)((E.G / E.dims[0]) / E.tl[0]);
   for (int a = 0; a < 4; ++a) E.tpi[a] = 1;
   for (int a = 1; a < E.ndim; ++a) {
-    const int64_t tiles = (E.G / E.dims[a]) / tile_lines_of(E.logn[a]);
-    int want = engine_env_int("PKDE_ENGINE_TPI", 2, 1, 16);
+    const int64_t tiles = (E.G / E.dims[a]) / E.tl[a];
+    // tiles per axis-pass item: 2 for 2-D, 8 for 3-D/4-D (measured on 128^3 / B = 32:
+    // 300 ms at 2, 267 ms at 4, 246 ms at 8)
+    int want = engine_env_int("PKDE_ENGINE_TPI", E.ndim == 2 ? 2 : 8, 1, 16);
     while (want > 1 && tiles % want) want >>= 1;
     E.tpi[a] = want;
   }
@@ -495,64 +713,173 @@ void run_engine(pkde_ctx *ctx, const EngineArgs &A, cudaStream_t st) {
   E.steps_low = A.steps_low;
   E.steps_over = A.steps_over;
   E.cs = A.cs;
-  for (int l = 0; l < 13; ++l) E.tw[l] = nullptr;
+  return E;
+}
+
+}  // namespace
+
+void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStream_t st) {
+  if (count < 1) return;
+  std::vector<EngineEst> est(count);
+  std::vector<std::vector<int64_t>> rs(count);
   size_t max_tile = 0, max_tw = 1;
-  for (int j = 0; j < g->ndim; ++j) {
-    E.tw[E.logn[j]] = stage_twiddles_device(ctx, E.logn[j]);
-    max_tile = std::max(max_tile, tile_elems(E.logn[j]));
-    max_tw = std::max(max_tw, tw_elems(E.logn[j]));
-  }
-  // schedule: items per round
-  std::vector<int64_t> rs(E.nrounds + 1, 0);
-  for (int64_t r = 0; r < E.nrounds; ++r) {
-    int64_t n = 0;
-    for (int p = 0; p < E.P; ++p) {
-      const int64_t b = r - (int64_t)p * E.D;
-      if (b >= 0 && b < E.NB) n += pass_tiles(E, b, p);
+  EngineRun R{};
+  for (int l = 0; l < 13; ++l) R.tw[l] = nullptr;
+  for (int e = 0; e < count; ++e) {
+    EngineEst &E = est[e];
+    E = describe(args[e]);
+    for (int j = 0; j < E.ndim; ++j) {
+      if (E.gen[j]) {
+        E.twg[j] = twiddles_device(ctx, (int)E.dims[j]);
+        E.plan[j] = make_plan((int)E.dims[j]);
+        max_tile = std::max(max_tile, (size_t)2 * E.tl[j] * (size_t)(E.dims[j] + 1));
+      } else {
+        R.tw[E.logn[j]] = stage_twiddles_device(ctx, E.logn[j]);
+        max_tile = std::max(max_tile, tile_elems(E.logn[j]));
+        max_tw = std::max(max_tw, tw_elems(E.logn[j]));
+      }
     }
-    rs[r + 1] = rs[r] + n;
+    // local schedule: items per round
+    std::vector<int64_t> &r = rs[e];
+    r.assign(E.nrounds + 1, 0);
+    for (int64_t k = 0; k < E.nrounds; ++k) {
+      int64_t n = 0;
+      for (int p = 0; p < E.P; ++p) {
+        const int64_t b = k - (int64_t)p * E.D;
+        if (b >= 0 && b < E.NB) n += pass_tiles(E, b, p);
+      }
+      r[k + 1] = r[k] + n;
+    }
   }
-  const int64_t total = rs[E.nrounds];
-  // device memory: [slots][wstate][per-step scalars][round starts][counters]
-  const size_t slot_bytes = sizeof(double2) * (size_t)E.Q * E.slot_elems;
-  const size_t wst_bytes = sizeof(double) * 4 * (size_t)E.G;
-  const size_t sc_bytes = sizeof(double) * 3 * (size_t)E.S;
-  const size_t rs_bytes = sizeof(int64_t) * rs.size();
-  const size_t cnt_bytes = sizeof(int) * ((size_t)E.NB * E.P + (size_t)E.NB * E.Tf + 2);
-  char *m = (char *)ensure(ctx, BUF_SCRATCH, slot_bytes + wst_bytes + sc_bytes + rs_bytes + cnt_bytes + 256);
-  E.slots = (double2 *)m;
-  E.wstate = (double *)(m + slot_bytes);
-  double *sc = (double *)(m + slot_bytes + wst_bytes);
-  int64_t *drs = (int64_t *)(m + slot_bytes + wst_bytes + sc_bytes);
-  int *cnt = (int *)(m + slot_bytes + wst_bytes + sc_bytes + rs_bytes);
-  E.cw = sc;
-  E.vscale = sc + E.S;
-  E.dlogt = sc + 2 * E.S;
-  E.round_start = drs;
-  E.cnt = cnt;
-  E.fin = cnt + E.NB * E.P;
-  E.next = E.fin + E.NB * E.Tf;
-  E.error = E.next + 1;
-  PKDE_CUDA_TRY(cudaMemcpyAsync(sc, A.cw, sizeof(double) * E.S, cudaMemcpyHostToDevice, st));
-  PKDE_CUDA_TRY(cudaMemcpyAsync(sc + E.S, A.vscale, sizeof(double) * E.S, cudaMemcpyHostToDevice, st));
-  PKDE_CUDA_TRY(cudaMemcpyAsync(sc + 2 * E.S, A.dlogt, sizeof(double) * E.S, cudaMemcpyHostToDevice, st));
-  PKDE_CUDA_TRY(cudaMemcpyAsync(drs, rs.data(), rs_bytes, cudaMemcpyHostToDevice, st));
-  PKDE_CUDA_TRY(cudaMemsetAsync(cnt, 0, cnt_bytes, st));
+  // Global schedule.  Estimations are dealt to `lanes` lanes in order (each to the lane
+  // that frees first); a lane runs its estimations one after another, lanes run side by
+  // side.  More lanes: more independent work per round; fewer: a smaller working set.
+  const int lanes = engine_env_int("PKDE_ENGINE_LANES", count, 1, 1 << 20);
+  std::vector<int64_t> start(count), lane_end(std::min(lanes, count), 0);
+  for (int e = 0; e < count; ++e) {
+    size_t best = 0;
+    for (size_t l = 1; l < lane_end.size(); ++l)
+      if (lane_end[l] < lane_end[best]) best = l;
+    start[e] = lane_end[best];
+    lane_end[best] += est[e].nrounds;
+  }
+  int64_t nglobal = 0;
+  for (int64_t v : lane_end) nglobal = std::max(nglobal, v);
+  std::vector<int64_t> seg_start;
+  std::vector<int2> seg;
+  {
+    // estimations active in each global round, in estimation order
+    std::vector<std::vector<int>> begin_at(nglobal + 1);
+    for (int e = 0; e < count; ++e) begin_at[start[e]].push_back(e);
+    std::vector<int> active;
+    int64_t cum = 0;
+    for (int64_t Rg = 0; Rg < nglobal; ++Rg) {
+      if (!begin_at[Rg].empty()) {
+        active.insert(active.end(), begin_at[Rg].begin(), begin_at[Rg].end());
+        std::sort(active.begin(), active.end());
+      }
+      size_t keep = 0;
+      for (size_t q = 0; q < active.size(); ++q) {
+        const int e = active[q];
+        const int64_t k = Rg - start[e];
+        const int64_t n = rs[e][k + 1] - rs[e][k];
+        if (n > 0) {
+          seg_start.push_back(cum);
+          seg.push_back(make_int2(e, (int)k));
+          cum += n;
+        }
+        if (k + 1 < est[e].nrounds) active[keep++] = e;
+      }
+      active.resize(keep);
+    }
+    seg_start.push_back(cum);
+  }
+  const int64_t nseg = (int64_t)seg.size();
+  const int64_t total = seg_start.back();
+
+  // device arena: [staged: descriptors | seg_start | seg | per estimation: scalars,
+  // round starts] [counters: per estimation cnt, fin | next, error] [per estimation:
+  // ring slots, Welford state]
+  size_t staged = 0;
+  const size_t off_est = staged;
+  staged = align256(staged + sizeof(EngineEst) * count);
+  const size_t off_segs = staged;
+  staged = align256(staged + sizeof(int64_t) * (nseg + 1));
+  const size_t off_seg = staged;
+  staged = align256(staged + sizeof(int2) * std::max<int64_t>(nseg, 1));
+  std::vector<size_t> off_sc(count), off_rs(count), off_cnt(count), off_slot(count);
+  for (int e = 0; e < count; ++e) {
+    off_sc[e] = staged;
+    staged = align256(staged + sizeof(double) * 3 * est[e].S);
+    off_rs[e] = staged;
+    staged = align256(staged + sizeof(int64_t) * rs[e].size());
+  }
+  size_t counters = staged;
+  for (int e = 0; e < count; ++e) {
+    off_cnt[e] = counters;
+    counters = align256(counters + sizeof(int) * ((size_t)est[e].NB * est[e].P + (size_t)est[e].NB * est[e].Tf));
+  }
+  const size_t off_flags = counters;
+  counters = align256(counters + 2 * sizeof(int));
+  size_t total_bytes = counters;
+  for (int e = 0; e < count; ++e) {
+    off_slot[e] = total_bytes;
+    total_bytes = align256(total_bytes + sizeof(double2) * (size_t)est[e].Q * est[e].slot_elems +
+                           sizeof(double) * 4 * (size_t)est[e].G);
+  }
+  char *m = (char *)ensure(ctx, BUF_ENGINE, total_bytes);
+  std::vector<char> host(staged, 0);
+  for (int e = 0; e < count; ++e) {
+    EngineEst &E = est[e];
+    double *sc = (double *)(m + off_sc[e]);
+    E.cw = sc;
+    E.vscale = sc + E.S;
+    E.dlogt = sc + 2 * E.S;
+    E.round_start = (const int64_t *)(m + off_rs[e]);
+    E.cnt = (int *)(m + off_cnt[e]);
+    E.fin = E.cnt + E.NB * E.P;
+    E.slots = (double2 *)(m + off_slot[e]);
+    E.wstate = (double *)(m + off_slot[e] + sizeof(double2) * (size_t)E.Q * E.slot_elems);
+    double *hsc = (double *)(host.data() + off_sc[e]);
+    std::memcpy(hsc, args[e].cw, sizeof(double) * E.S);
+    std::memcpy(hsc + E.S, args[e].vscale, sizeof(double) * E.S);
+    std::memcpy(hsc + 2 * E.S, args[e].dlogt, sizeof(double) * E.S);
+    std::memcpy(host.data() + off_rs[e], rs[e].data(), sizeof(int64_t) * rs[e].size());
+  }
+  std::memcpy(host.data() + off_est, est.data(), sizeof(EngineEst) * count);
+  std::memcpy(host.data() + off_segs, seg_start.data(), sizeof(int64_t) * (nseg + 1));
+  if (nseg) std::memcpy(host.data() + off_seg, seg.data(), sizeof(int2) * nseg);
+  PKDE_CUDA_TRY(cudaMemcpyAsync(m, host.data(), staged, cudaMemcpyHostToDevice, st));
+  PKDE_CUDA_TRY(cudaMemsetAsync(m + staged, 0, counters - staged, st));
+  R.est = (const EngineEst *)(m + off_est);
+  R.count = count;
+  R.seg_start = (const int64_t *)(m + off_segs);
+  R.seg = (const int2 *)(m + off_seg);
+  R.nseg = nseg;
+  R.total_items = total;
+  R.next = (int *)(m + off_flags);
+  R.error = R.next + 1;
+  bool any_gen = false;
+  for (int e = 0; e < count; ++e)
+    for (int j = 0; j < est[e].ndim; ++j) any_gen |= est[e].gen[j] != 0;
+  auto kern = any_gen ? engine_kernel<true> : engine_kernel<false>;
   const size_t smem = sizeof(double2) * (max_tile + 8 * kEngineThreads + max_tw);
-  PKDE_CUDA_TRY(cudaFuncSetAttribute(engine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PKDE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  PKDE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_kernel, kEngineThreads, smem));
+  PKDE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEngineThreads, smem));
   if (per_sm < 1) throw Error{PKDE_EUNSUPPORTED, "engine kernel does not fit on an SM"};
   const int64_t grid = std::min<int64_t>(total, (int64_t)per_sm * ctx->sm_count);
-  {
+  if (grid > 0) {
     Trace tr(ctx, PKDE_PHASE_STEP_VMR, st);
-    engine_kernel<<<(unsigned)grid, kEngineThreads, smem, st>>>(E, total, (int)max_tile, (int)max_tw);
+    kern<<<(unsigned)grid, kEngineThreads, smem, st>>>(R, (int)max_tile);
   }
   PKDE_CHECK_LAUNCH();
   int err = 0;
-  PKDE_CUDA_TRY(cudaMemcpyAsync(&err, E.error, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PKDE_CUDA_TRY(cudaMemcpyAsync(&err, R.error, sizeof(int), cudaMemcpyDeviceToHost, st));
   PKDE_CUDA_TRY(cudaStreamSynchronize(st));
   if (err) throw Error{PKDE_ECUDA, "step engine: a dependency wait timed out (run aborted)"};
 }
+
+void run_engine(pkde_ctx *ctx, const EngineArgs &A, cudaStream_t st) { run_engine_batch(ctx, &A, 1, st); }
 
 }  // namespace pkde

@@ -23,8 +23,6 @@
 
 namespace pkde {
 
-void dirac_paired(pkde_ctx *ctx, const pkde_grid *g, const double *d_data, int64_t n, const int32_t *d_idx,
-                  int64_t nboot, uint64_t seed, double2 *spectra, cudaStream_t st);
 int lines_per_cta(int n, int64_t nlines);
 
 namespace {
@@ -214,25 +212,43 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return t;
 }
 
-__global__ void moments_partial_kernel(const double *data, int64_t n, int ndim, const double *mean, double *partial) {
+// Sums over the samples of one estimation per blockIdx.y: per axis, of x (mean ==
+// nullptr) or of (x - mean)^2.  Each of the job's nb blocks writes its partial sums
+// (fixed tree order); moments_final_kernel adds a job's partials in order.  The
+// partition depends only on the job's own n, so an estimation gets the same sums alone
+// and in a batch.
+struct MomentJob {
+  const double *data;
+  int64_t n;
+  int ndim;
+  int nb;
+  double *partial;     // nb x ndim
+  const double *mean;  // ndim, or nullptr
+  double *out;         // ndim
+};
+
+__global__ void moments_partial_kernel(const MomentJob *jobs) {
   __shared__ double sh[32];
-  for (int j = 0; j < ndim; ++j) {
-    const double mu = mean ? mean[j] : 0.0;
+  const MomentJob J = jobs[blockIdx.y];
+  if ((int)blockIdx.x >= J.nb) return;  // uniform over the block
+  for (int j = 0; j < J.ndim; ++j) {
+    const double mu = J.mean ? J.mean[j] : 0.0;
     double s = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-      const double x = data[i * ndim + j];
-      s += mean ? (x - mu) * (x - mu) : x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < J.n; i += (int64_t)J.nb * blockDim.x) {
+      const double x = J.data[i * J.ndim + j];
+      s += J.mean ? (x - mu) * (x - mu) : x;
     }
     const double t = block_sum(s, sh);
-    if (threadIdx.x == 0) partial[blockIdx.x * ndim + j] = t;
+    if (threadIdx.x == 0) J.partial[blockIdx.x * J.ndim + j] = t;
   }
 }
 
-__global__ void moments_final_kernel(const double *partial, int nblocks, int ndim, double *out) {
-  if (threadIdx.x < ndim) {
+__global__ void moments_final_kernel(const MomentJob *jobs) {
+  const MomentJob J = jobs[blockIdx.x];
+  if ((int)threadIdx.x < J.ndim) {
     double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partial[b * ndim + threadIdx.x];
-    out[threadIdx.x] = s;
+    for (int b = 0; b < J.nb; ++b) s += J.partial[b * J.ndim + threadIdx.x];
+    J.out[threadIdx.x] = s;
   }
 }
 
@@ -335,41 +351,61 @@ Ladder make_ladder(const pkde_gradepro_params *p, const double *bw_final, int64_
   return L;
 }
 
-// Silverman's rule (DirectSpace.jl:1102-1111) from FP64 device moments.
-static void silverman_device(pkde_ctx *ctx, const double *d_data, int64_t n, int N, double *bw, cudaStream_t st) {
-  const int nb = blocks_for(ctx, n);
-  double *m = (double *)ensure(ctx, BUF_MISC, sizeof(double) * (16 + 4 * (size_t)nb));
-  double *sum = m, *cen = m + 4, *meanv = m + 8, *partial = m + 16;
-  {
-    ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-    moments_partial_kernel<<<nb, kThreads, 0, st>>>(d_data, n, N, nullptr, partial);
+// Silverman's rule (DirectSpace.jl:1102-1111) from FP64 device moments, for several
+// estimations at once: two reductions, two read-backs for the whole set.
+//   data[e], n[e], N[e] -> bw[4e .. 4e+N[e]-1]
+static void silverman_batch(pkde_ctx *ctx, int count, const double *const *data, const int64_t *n, const int *N,
+                            double *bw, cudaStream_t st) {
+  if (count < 1) return;
+  std::vector<MomentJob> jobs(count);
+  int maxnb = 1;
+  size_t npart = 0;
+  for (int e = 0; e < count; ++e) {
+    jobs[e].nb = blocks_for(ctx, n[e]);
+    maxnb = std::max(maxnb, jobs[e].nb);
+    npart += 4 * (size_t)jobs[e].nb;
   }
-  PKDE_CHECK_LAUNCH();
-  {
-    ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-    moments_final_kernel<<<1, 32, 0, st>>>(partial, nb, N, sum);
+  // device: [jobs][sums count x 4][means count x 4][partials]
+  const size_t jb = (sizeof(MomentJob) * count + 255) & ~size_t(255);
+  char *m = (char *)ensure(ctx, BUF_MISC, jb + sizeof(double) * (8 * (size_t)count + npart));
+  MomentJob *djobs = (MomentJob *)m;
+  double *sums = (double *)(m + jb), *means = sums + 4 * count, *partial = means + 4 * count;
+  for (int e = 0; e < count; ++e) {
+    jobs[e].data = data[e];
+    jobs[e].n = n[e];
+    jobs[e].ndim = N[e];
+    jobs[e].partial = partial;
+    partial += 4 * (size_t)jobs[e].nb;
+    jobs[e].mean = nullptr;
+    jobs[e].out = sums + 4 * e;
   }
-  PKDE_CHECK_LAUNCH();
-  double h[4];
-  PKDE_CUDA_TRY(cudaMemcpyAsync(h, sum, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
-  PKDE_CUDA_TRY(cudaStreamSynchronize(st));
-  for (int j = 0; j < N; ++j) h[j] /= (double)n;
-  PKDE_CUDA_TRY(cudaMemcpyAsync(meanv, h, sizeof(double) * N, cudaMemcpyHostToDevice, st));
-  {
-    ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-    moments_partial_kernel<<<nb, kThreads, 0, st>>>(d_data, n, N, meanv, partial);
+  std::vector<double> h(4 * (size_t)count);
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1)
+      for (int e = 0; e < count; ++e) jobs[e].mean = means + 4 * e;
+    PKDE_CUDA_TRY(cudaMemcpyAsync(djobs, jobs.data(), sizeof(MomentJob) * count, cudaMemcpyHostToDevice, st));
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+      moments_partial_kernel<<<dim3((unsigned)maxnb, (unsigned)count), kThreads, 0, st>>>(djobs);
+    }
+    PKDE_CHECK_LAUNCH();
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+      moments_final_kernel<<<(unsigned)count, 32, 0, st>>>(djobs);
+    }
+    PKDE_CHECK_LAUNCH();
+    PKDE_CUDA_TRY(cudaMemcpyAsync(h.data(), sums, sizeof(double) * 4 * count, cudaMemcpyDeviceToHost, st));
+    PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+    if (pass == 0) {
+      for (int e = 0; e < count; ++e)
+        for (int j = 0; j < N[e]; ++j) h[4 * e + j] /= (double)n[e];
+      PKDE_CUDA_TRY(cudaMemcpyAsync(means, h.data(), sizeof(double) * 4 * count, cudaMemcpyHostToDevice, st));
+    }
   }
-  PKDE_CHECK_LAUNCH();
-  {
-    ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-    moments_final_kernel<<<1, 32, 0, st>>>(partial, nb, N, cen);
+  for (int e = 0; e < count; ++e) {
+    const double pref = std::pow(4.0 / ((double)(N[e] + 2) * (double)n[e]), 1.0 / (double)(N[e] + 4));
+    for (int j = 0; j < N[e]; ++j) bw[4 * e + j] = pref * std::sqrt(h[4 * e + j] / (double)(n[e] - 1));
   }
-  PKDE_CHECK_LAUNCH();
-  double c[4];
-  PKDE_CUDA_TRY(cudaMemcpyAsync(c, cen, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
-  PKDE_CUDA_TRY(cudaStreamSynchronize(st));
-  const double pref = std::pow(4.0 / ((double)(N + 2) * (double)n), 1.0 / (double)(N + 4));
-  for (int j = 0; j < N; ++j) bw[j] = pref * std::sqrt(c[j] / (double)(n - 1));
 }
 
 // Per-step, per-axis propagation factors: p(k) = exp(-0.5 (k t)^2) and sqrt(p(k)),
@@ -409,43 +445,44 @@ static void set_smem(K kernel, size_t bytes) {
   PKDE_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
-// The plain one-estimation-at-a-time pipeline.
+// One estimation of a call (device pointers).
 struct Estimation {
   const pkde_gradepro_params *p;
   int64_t n;
   const double *d_data;
   const int32_t *d_idx;
   uint64_t seed;
+  double *d_density;    // may be null
+  int32_t *d_selected;  // may be null
 };
 
-void run_gradepro(pkde_ctx *ctx, const Estimation &E, double *d_density, int32_t *d_selected, cudaStream_t st) {
-  const pkde_gradepro_params *p = E.p;
-  const pkde_grid *g = &p->grid;
-  const int N = g->ndim;
-  const int64_t G = grid_size(g);
-  const int64_t B = p->n_bootstraps;
-  const int64_t npairs = (B + 1) / 2;
-  const int n1 = (int)g->dims[0];
-  const int64_t rows = G / n1;
+enum class StepPath { Steps1D, Engine, Generic };
 
-  // bandwidth ladder (host), Silverman from device moments when bw_final is NaN
-  double bw[4];
-  bool need_silverman = false;
-  for (int j = 0; j < N; ++j) need_silverman |= std::isnan(p->bw_final[j]);
-  if (need_silverman) silverman_device(ctx, E.d_data, E.n, N, bw, st);
-  for (int j = 0; j < N; ++j)
-    if (!std::isnan(p->bw_final[j])) bw[j] = p->bw_final[j];
-  Ladder L = make_ladder(p, bw, E.n);
+// Everything the device work of one estimation needs.
+struct Plan {
+  const Estimation *E;
+  const pkde_grid *g;
+  int N;
+  int64_t G, B, npairs;
+  StepPath path;
+  Ladder L;
+  std::vector<double> fz, fw;
+  std::vector<int64_t> aoff;
+  int64_t tot;
+  // device buffers (in the call's arena)
+  double2 *spectra;
+  ConvState cs;
+  double *tables;    // fz tables then fw tables, S x tot each
+  double *per_step;  // 1-D: f (S x G), mu (S x G), cw, vscale, dlogt (S each)
+  char *bin_scratch;
+  int *misc;         // 256-byte block for the binning's flags and max count
+  DiracJob job;
+};
 
-  // device buffers
-  double2 *spectra = (double2 *)ensure(ctx, BUF_SPECTRA, sizeof(double2) * (2 * npairs + 1) * G);
-  const int64_t pair_bytes = (int64_t)sizeof(double2) * 2 * G;
-  int64_t group = std::max<int64_t>(1, std::min<int64_t>(npairs, (48ll << 20) / pair_bytes));
-  if (N == 1) group = npairs;
-  double2 *scratch = (double2 *)ensure(ctx, BUF_SCRATCH, N > 1 ? (size_t)pair_bytes * group : 16);
-  double *wel = (double *)ensure(ctx, BUF_WELFORD, sizeof(double) * 2 * G);
-  double *wmean = wel, *wm2 = wel + G;
-  char *stb = (char *)ensure(ctx, BUF_STATE, (sizeof(double) * 5 + sizeof(uint16_t) * 2 + 1 + 4) * G + 256);
+static size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+static size_t state_bytes(int64_t G) { return al256((sizeof(double) * 5 + sizeof(uint16_t) * 2 + 1 + 4) * G + 256); }
+
+static ConvState bind_state(char *stb, int64_t G) {
   ConvState cs;
   cs.f1 = (double *)stb;
   cs.f2 = cs.f1 + G;
@@ -456,77 +493,32 @@ void run_gradepro(pkde_ctx *ctx, const Estimation &E, double *d_density, int32_t
   cs.c_low = (uint16_t *)(cs.selected + G);
   cs.c_over = cs.c_low + G;
   cs.flags = (uint8_t *)(cs.c_over + G);
+  return cs;
+}
 
-  std::vector<double> fz, fw;
-  std::vector<int64_t> aoff;
-  factor_tables(g, L, fz, fw, aoff);
-  const int64_t tot = aoff[N];
-  double *tables = (double *)ensure(ctx, BUF_TABLES, sizeof(double) * 2 * L.S * tot);
-  PKDE_CUDA_TRY(cudaMemcpyAsync(tables, fz.data(), sizeof(double) * L.S * tot, cudaMemcpyHostToDevice, st));
-  PKDE_CUDA_TRY(cudaMemcpyAsync(tables + L.S * tot, fw.data(), sizeof(double) * L.S * tot, cudaMemcpyHostToDevice, st));
-  const double *dfz = tables, *dfw = tables + L.S * tot;
-
-  // binning into the paired layout, forward FFT of every array
-  dirac_paired(ctx, g, E.d_data, E.n, E.d_idx, B, E.seed, spectra, st);
-  fft_nd(ctx, N, g->dims, spectra, 2 * npairs + 1, -1, st, PKDE_PHASE_FORWARD_FFT);
-
-  if (steps1d_ok(g)) {
-    // 1-D: every bandwidth step in parallel (one CTA each), then the convergence
-    // state machine over the stored per-step f_s and means.
-    const int64_t S = L.S;
-    double *per_step = (double *)ensure(ctx, BUF_SCRATCH, sizeof(double) * (2 * S * G + 3 * S));
-    double *f_all = per_step, *mu_all = per_step + S * G;
-    double *d_cw = mu_all + S * G, *d_vs = d_cw + S, *d_dl = d_vs + S;
-    PKDE_CUDA_TRY(cudaMemcpyAsync(d_cw, L.cw.data(), sizeof(double) * S, cudaMemcpyHostToDevice, st));
-    PKDE_CUDA_TRY(cudaMemcpyAsync(d_vs, L.vscale.data(), sizeof(double) * S, cudaMemcpyHostToDevice, st));
-    PKDE_CUDA_TRY(cudaMemcpyAsync(d_dl, L.dlogt.data(), sizeof(double) * S, cudaMemcpyHostToDevice, st));
-    steps1d(ctx, n1, spectra, (int)npairs, (int)B, (int)S, dfz, dfw, tot, d_cw, 1.0 / (double)G, 1.0 / (double)E.n,
-            d_vs, f_all, mu_all, st);
-    converge_steps(ctx, G, (int)S, f_all, mu_all, d_dl, L.eps, L.steps_low, L.steps_over, cs, st);
-    if (d_density) PKDE_CUDA_TRY(cudaMemcpyAsync(d_density, cs.density, sizeof(double) * G, cudaMemcpyDeviceToDevice, st));
-    if (d_selected)
-      PKDE_CUDA_TRY(cudaMemcpyAsync(d_selected, cs.selected, sizeof(int32_t) * G, cudaMemcpyDeviceToDevice, st));
-    return;
-  }
-
-  {
-    ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-    init_state_kernel<<<blocks_for(ctx, G), kThreads, 0, st>>>(G, cs);
-  }
-  PKDE_CHECK_LAUNCH();
-
-  if (engine_ok(g)) {
-    // N-D on power-of-two axes: the persistent step engine runs every bandwidth step
-    EngineArgs A{};
-    A.grid = g;
-    A.npairs = (int)npairs;
-    A.nboot = (int)B;
-    A.S = (int)L.S;
-    A.spectra = spectra;
-    A.fz = dfz;
-    A.fw = dfw;
-    A.tab_stride = tot;
-    for (int j = 0; j < N; ++j) A.aoff[j] = aoff[j];
-    A.cw = L.cw.data();
-    A.vscale = L.vscale.data();
-    A.dlogt = L.dlogt.data();
-    A.inv_n = 1.0 / (double)E.n;
-    A.eps = L.eps;
-    A.steps_low = L.steps_low;
-    A.steps_over = L.steps_over;
-    A.cs = cs;
-    run_engine(ctx, A, st);
-    {
-      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-      replace_nans_kernel<<<blocks_for(ctx, G), kThreads, 0, st>>>(G, cs, (int)L.S);
-    }
-    PKDE_CHECK_LAUNCH();
-    if (d_density) PKDE_CUDA_TRY(cudaMemcpyAsync(d_density, cs.density, sizeof(double) * G, cudaMemcpyDeviceToDevice, st));
-    if (d_selected)
-      PKDE_CUDA_TRY(cudaMemcpyAsync(d_selected, cs.selected, sizeof(int32_t) * G, cudaMemcpyDeviceToDevice, st));
-    return;
-  }
-
+// Bandwidth steps of an N-D estimation on the launch-based path (any axis lengths):
+// per step and pair group, inverse FFT passes over axes N..2 then the fused axis-1 pass
+// with VMR + Welford, then the means pass with the convergence update.
+static void run_generic(pkde_ctx *ctx, Plan &P, cudaStream_t st) {
+  const Estimation &E = *P.E;
+  const pkde_grid *g = P.g;
+  const int N = P.N;
+  const int64_t G = P.G;
+  const int64_t B = P.B;
+  const int64_t npairs = P.npairs;
+  const int n1 = (int)g->dims[0];
+  const int64_t rows = G / n1;
+  const Ladder &L = P.L;
+  const std::vector<int64_t> &aoff = P.aoff;
+  const int64_t tot = P.tot;
+  double2 *spectra = P.spectra;
+  ConvState cs = P.cs;
+  const double *dfz = P.tables, *dfw = P.tables + L.S * tot;
+  const int64_t pair_bytes = (int64_t)sizeof(double2) * 2 * G;
+  const int64_t group = std::max<int64_t>(1, std::min<int64_t>(npairs, (48ll << 20) / pair_bytes));
+  double2 *scratch = (double2 *)ensure(ctx, BUF_SCRATCH, (size_t)pair_bytes * group);
+  double *wel = (double *)ensure(ctx, BUF_WELFORD, sizeof(double) * 2 * G);
+  double *wmean = wel, *wm2 = wel + G;
   // final-pass geometry
   int tl = std::max(1, std::min<int>(2048 / n1, 16));
   if (tl > rows) tl = (int)rows;
@@ -624,14 +616,202 @@ void run_gradepro(pkde_ctx *ctx, const Estimation &E, double *d_density, int32_t
     else
       launch_means(msrc, fzs + aoff[0], invG, s);
   }
-  {
-    ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-    replace_nans_kernel<<<blocks_for(ctx, G), kThreads, 0, st>>>(G, cs, (int)L.S);
+}
+
+static void make_plan_tables(Plan &P) {
+  factor_tables(P.g, P.L, P.fz, P.fw, P.aoff);
+  P.tot = P.aoff[P.N];
+}
+
+// The :gradepro estimation of `count` independent sample sets on one stream: each phase
+// runs for every estimation before the next phase starts, so the whole call has one
+// host synchronisation per phase (Silverman moments, binning read-back), and the
+// bandwidth steps of all N-D power-of-two estimations run in one persistent launch.
+// An estimation gets the same result alone and in a batch: every kernel partitions its
+// work by the estimation's own sizes only.
+void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st) {
+  std::vector<Plan> plans(count);
+  // ---- Silverman's rule where bw_final is NaN
+  std::vector<const double *> sd;
+  std::vector<int64_t> sn;
+  std::vector<int> sN, who;
+  for (int e = 0; e < count; ++e) {
+    Plan &P = plans[e];
+    P.E = &ests[e];
+    P.g = &ests[e].p->grid;
+    P.N = P.g->ndim;
+    P.G = grid_size(P.g);
+    P.B = ests[e].p->n_bootstraps;
+    P.npairs = (P.B + 1) / 2;
+    bool need = false;
+    for (int j = 0; j < P.N; ++j) need |= std::isnan(ests[e].p->bw_final[j]);
+    if (need) {
+      sd.push_back(ests[e].d_data);
+      sn.push_back(ests[e].n);
+      sN.push_back(P.N);
+      who.push_back(e);
+    }
   }
-  PKDE_CHECK_LAUNCH();
-  if (d_density) PKDE_CUDA_TRY(cudaMemcpyAsync(d_density, cs.density, sizeof(double) * G, cudaMemcpyDeviceToDevice, st));
-  if (d_selected)
-    PKDE_CUDA_TRY(cudaMemcpyAsync(d_selected, cs.selected, sizeof(int32_t) * G, cudaMemcpyDeviceToDevice, st));
+  std::vector<double> sbw(4 * sd.size());
+  silverman_batch(ctx, (int)sd.size(), sd.data(), sn.data(), sN.data(), sbw.data(), st);
+  // ---- ladders, factor tables, paths
+  size_t arena = al256(256 * (size_t)count);  // misc blocks first (one read-back)
+  size_t tables_bytes = 0;
+  size_t generic_wel = 0, generic_scr = 0;
+  std::vector<size_t> off(count);
+  for (int e = 0, k = 0; e < count; ++e) {
+    Plan &P = plans[e];
+    double bw[4];
+    const bool need = k < (int)who.size() && who[k] == e;
+    for (int j = 0; j < P.N; ++j) bw[j] = need ? sbw[4 * k + j] : 0.0;
+    if (need) ++k;
+    for (int j = 0; j < P.N; ++j)
+      if (!std::isnan(ests[e].p->bw_final[j])) bw[j] = ests[e].p->bw_final[j];
+    P.L = make_ladder(ests[e].p, bw, ests[e].n);
+    make_plan_tables(P);
+    P.path = steps1d_ok(P.g) ? StepPath::Steps1D : (engine_ok(P.g) ? StepPath::Engine : StepPath::Generic);
+    if (ctx->step_path == PKDE_STEPS_PER_STEP_LAUNCH) P.path = StepPath::Generic;
+    tables_bytes += al256(sizeof(double) * 2 * P.L.S * P.tot);
+  }
+  // arena: [misc blocks][tables of every estimation][per estimation: spectra, state,
+  // 1-D per-step arrays, binning scratch]
+  const size_t off_tables = arena;
+  arena += tables_bytes;
+  for (int e = 0; e < count; ++e) {
+    Plan &P = plans[e];
+    off[e] = arena;
+    arena += al256(sizeof(double2) * (2 * P.npairs + 1) * P.G);
+    arena += state_bytes(P.G);
+    if (P.path == StepPath::Steps1D) arena += al256(sizeof(double) * (2 * P.L.S * P.G + 3 * P.L.S));
+    arena += dirac_job_scratch(P.g, ests[e].n, P.B);
+    if (P.path == StepPath::Generic) {
+      generic_wel = std::max(generic_wel, sizeof(double) * 2 * (size_t)P.G);
+      const int64_t pair_bytes = (int64_t)sizeof(double2) * 2 * P.G;
+      const int64_t group = std::max<int64_t>(1, std::min<int64_t>(P.npairs, (48ll << 20) / pair_bytes));
+      generic_scr = std::max(generic_scr, (size_t)(pair_bytes * group));
+    }
+  }
+  char *base = (char *)ensure(ctx, BUF_BATCH, arena);
+  if (generic_scr) {  // sized once, so that no buffer grows while kernels are queued
+    ensure(ctx, BUF_SCRATCH, generic_scr);
+    ensure(ctx, BUF_WELFORD, generic_wel);
+  }
+  std::vector<char> htab(tables_bytes);
+  size_t toff = 0;
+  for (int e = 0; e < count; ++e) {
+    Plan &P = plans[e];
+    const int64_t S = P.L.S;
+    P.misc = (int *)(base + 256 * (size_t)e);
+    P.tables = (double *)(base + off_tables + toff);
+    std::memcpy(htab.data() + toff, P.fz.data(), sizeof(double) * S * P.tot);
+    std::memcpy(htab.data() + toff + sizeof(double) * S * P.tot, P.fw.data(), sizeof(double) * S * P.tot);
+    toff += al256(sizeof(double) * 2 * S * P.tot);
+    char *q = base + off[e];
+    P.spectra = (double2 *)q;
+    q += al256(sizeof(double2) * (2 * P.npairs + 1) * P.G);
+    P.cs = bind_state(q, P.G);
+    q += state_bytes(P.G);
+    P.per_step = nullptr;
+    if (P.path == StepPath::Steps1D) {
+      P.per_step = (double *)q;
+      q += al256(sizeof(double) * (2 * S * P.G + 3 * S));
+    }
+    P.bin_scratch = q;
+    P.job.g = P.g;
+    P.job.d_data = ests[e].d_data;
+    P.job.n = ests[e].n;
+    P.job.d_idx = ests[e].d_idx;
+    P.job.nboot = P.B;
+    P.job.seed = ests[e].seed;
+    P.job.paired_out = P.spectra;
+    dirac_job_bind(P.job, P.bin_scratch, P.misc);
+  }
+  if (tables_bytes)
+    PKDE_CUDA_TRY(cudaMemcpyAsync(base + off_tables, htab.data(), tables_bytes, cudaMemcpyHostToDevice, st));
+  // ---- binning: phase A for all, one read-back, phase B for all
+  for (int e = 0; e < count; ++e) dirac_job_phase_a(ctx, plans[e].job, st);
+  std::vector<int> hmisc(64 * (size_t)count);
+  PKDE_CUDA_TRY(cudaMemcpyAsync(hmisc.data(), base, 256 * (size_t)count, cudaMemcpyDeviceToHost, st));
+  PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int e = 0; e < count; ++e) {
+    try {
+      dirac_job_phase_b(ctx, plans[e].job, &hmisc[64 * (size_t)e], st);
+    } catch (Error &err) {
+      if (count > 1) err.msg = "estimation " + std::to_string(e) + ": " + err.msg;
+      throw;
+    }
+  }
+  // ---- forward FFT of every array
+  for (int e = 0; e < count; ++e)
+    fft_nd(ctx, plans[e].N, plans[e].g->dims, plans[e].spectra, 2 * plans[e].npairs + 1, -1, st,
+           PKDE_PHASE_FORWARD_FFT);
+  // ---- bandwidth steps
+  std::vector<EngineArgs> eng;
+  std::vector<int> eng_who;
+  for (int e = 0; e < count; ++e) {
+    Plan &P = plans[e];
+    const Ladder &L = P.L;
+    const int64_t S = L.S;
+    const double *dfz = P.tables, *dfw = P.tables + S * P.tot;
+    if (P.path == StepPath::Steps1D) {
+      // 1-D: every bandwidth step in parallel (one CTA each), then the convergence
+      // state machine over the stored per-step f_s and means.
+      double *f_all = P.per_step, *mu_all = P.per_step + S * P.G;
+      double *d_cw = mu_all + S * P.G, *d_vs = d_cw + S, *d_dl = d_vs + S;
+      PKDE_CUDA_TRY(cudaMemcpyAsync(d_cw, L.cw.data(), sizeof(double) * S, cudaMemcpyHostToDevice, st));
+      PKDE_CUDA_TRY(cudaMemcpyAsync(d_vs, L.vscale.data(), sizeof(double) * S, cudaMemcpyHostToDevice, st));
+      PKDE_CUDA_TRY(cudaMemcpyAsync(d_dl, L.dlogt.data(), sizeof(double) * S, cudaMemcpyHostToDevice, st));
+      steps1d(ctx, (int)P.g->dims[0], P.spectra, (int)P.npairs, (int)P.B, (int)S, dfz, dfw, P.tot, d_cw,
+              1.0 / (double)P.G, 1.0 / (double)ests[e].n, d_vs, f_all, mu_all, st);
+      converge_steps(ctx, P.G, (int)S, f_all, mu_all, d_dl, L.eps, L.steps_low, L.steps_over, P.cs, st);
+      continue;
+    }
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+      init_state_kernel<<<blocks_for(ctx, P.G), kThreads, 0, st>>>(P.G, P.cs);
+    }
+    PKDE_CHECK_LAUNCH();
+    if (P.path == StepPath::Generic) {
+      run_generic(ctx, P, st);
+      continue;
+    }
+    // N-D on power-of-two axes: the persistent step engine
+    EngineArgs A{};
+    A.grid = P.g;
+    A.npairs = (int)P.npairs;
+    A.nboot = (int)P.B;
+    A.S = (int)S;
+    A.spectra = P.spectra;
+    A.fz = dfz;
+    A.fw = dfw;
+    A.tab_stride = P.tot;
+    for (int j = 0; j < P.N; ++j) A.aoff[j] = P.aoff[j];
+    A.cw = L.cw.data();
+    A.vscale = L.vscale.data();
+    A.dlogt = L.dlogt.data();
+    A.inv_n = 1.0 / (double)ests[e].n;
+    A.eps = L.eps;
+    A.steps_low = L.steps_low;
+    A.steps_over = L.steps_over;
+    A.cs = P.cs;
+    eng.push_back(A);
+    eng_who.push_back(e);
+  }
+  if (!eng.empty()) run_engine_batch(ctx, eng.data(), (int)eng.size(), st);
+  // ---- replace_nans! and outputs
+  for (int e = 0; e < count; ++e) {
+    Plan &P = plans[e];
+    if (P.path != StepPath::Steps1D) {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+      replace_nans_kernel<<<blocks_for(ctx, P.G), kThreads, 0, st>>>(P.G, P.cs, (int)P.L.S);
+    }
+    PKDE_CHECK_LAUNCH();
+    if (ests[e].d_density)
+      PKDE_CUDA_TRY(cudaMemcpyAsync(ests[e].d_density, P.cs.density, sizeof(double) * P.G, cudaMemcpyDeviceToDevice, st));
+    if (ests[e].d_selected)
+      PKDE_CUDA_TRY(
+          cudaMemcpyAsync(ests[e].d_selected, P.cs.selected, sizeof(int32_t) * P.G, cudaMemcpyDeviceToDevice, st));
+  }
 }
 
 static void validate_params(const pkde_gradepro_params *p, int64_t n) {
@@ -649,44 +829,93 @@ extern "C" {
 int pkde_gradepro_estimate(pkde_ctx *ctx, const pkde_gradepro_params *p, const double *data, int64_t n,
                            const int32_t *boot_idx, uint64_t seed, double *density_out, int32_t *selected_out,
                            uint32_t flags, void *stream) {
+  const double *d[1] = {data};
+  const int32_t *i[1] = {boot_idx};
+  double *o[1] = {density_out};
+  int32_t *so[1] = {selected_out};
+  return pkde_gradepro_estimate_batch(ctx, 1, p, d, &n, i, &seed, o, so, flags, stream);
+}
+
+int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradepro_params *params,
+                                 const double *const *data, const int64_t *n, const int32_t *const *boot_idx,
+                                 const uint64_t *seeds, double *const *density_out, int32_t *const *selected_out,
+                                 uint32_t flags, void *stream) {
   return pkde_guard(ctx, [&] {
     using namespace pkde;
     if (!ctx) throw invalid("context is NULL");
-    validate_params(p, n);
-    if (!data) throw invalid("data is NULL");
+    if (count < 1 || count > 65535) throw invalid("count must be in 1..65535 (got %d)", count);
+    if (!params || !data || !n) throw invalid("params, data and n are required");
+    for (int e = 0; e < count; ++e) {
+      validate_params(&params[e], n[e]);
+      if (!data[e]) throw invalid("data[%d] is NULL", e);
+    }
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
     cudaStream_t st = (cudaStream_t)stream;
-    const int N = p->grid.ndim;
-    const int64_t G = grid_size(&p->grid);
     const bool din = flags & PKDE_DEVICE_INPUT, dout = flags & PKDE_DEVICE_OUTPUT;
-    const double *d_data = data;
-    if (!din) {
-      double *dd = (double *)ensure(ctx, BUF_DATA, sizeof(double) * N * n);
-      copy_in(dd, data, sizeof(double) * N * n, false, st);
-      d_data = dd;
+    // host inputs: one device buffer for all samples (and one for all indices)
+    std::vector<size_t> doff(count), ioff(count), ooff(count);
+    size_t dbytes = 0, ibytes = 0, obytes = 0;
+    for (int e = 0; e < count; ++e) {
+      const int N = params[e].grid.ndim;
+      const int64_t G = grid_size(&params[e].grid);
+      doff[e] = dbytes;
+      dbytes += al256(sizeof(double) * N * n[e]);
+      ioff[e] = ibytes;
+      if (boot_idx && boot_idx[e]) ibytes += al256(sizeof(int32_t) * n[e] * params[e].n_bootstraps);
+      ooff[e] = obytes;
+      obytes += al256((sizeof(double) + sizeof(int32_t)) * G);
     }
-    const int32_t *d_idx = boot_idx;
-    if (boot_idx && !din) {
-      int32_t *di = (int32_t *)ensure(ctx, BUF_IDX, sizeof(int32_t) * n * p->n_bootstraps);
-      copy_in(di, boot_idx, sizeof(int32_t) * n * p->n_bootstraps, false, st);
-      d_idx = di;
+    char *ddata = din ? nullptr : (char *)ensure(ctx, BUF_DATA, dbytes);
+    char *didx = (din || !ibytes) ? nullptr : (char *)ensure(ctx, BUF_IDX, ibytes);
+    char *dout_buf = dout ? nullptr : (char *)ensure(ctx, BUF_OUT, obytes);
+    std::vector<Estimation> ests(count);
+    for (int e = 0; e < count; ++e) {
+      const int N = params[e].grid.ndim;
+      const int64_t G = grid_size(&params[e].grid);
+      Estimation &E = ests[e];
+      E.p = &params[e];
+      E.n = n[e];
+      E.seed = seeds ? seeds[e] : 0;
+      E.d_data = data[e];
+      if (!din) {
+        copy_in(ddata + doff[e], data[e], sizeof(double) * N * n[e], false, st);
+        E.d_data = (const double *)(ddata + doff[e]);
+      }
+      E.d_idx = (boot_idx && boot_idx[e]) ? boot_idx[e] : nullptr;
+      if (E.d_idx && !din) {
+        copy_in(didx + ioff[e], boot_idx[e], sizeof(int32_t) * n[e] * params[e].n_bootstraps, false, st);
+        E.d_idx = (const int32_t *)(didx + ioff[e]);
+      }
+      double *dens = density_out ? density_out[e] : nullptr;
+      int32_t *sel = selected_out ? selected_out[e] : nullptr;
+      if (!dout) {
+        dens = dens ? (double *)(dout_buf + ooff[e]) : nullptr;
+        sel = sel ? (int32_t *)(dout_buf + ooff[e] + sizeof(double) * G) : nullptr;
+      }
+      E.d_density = dens;
+      E.d_selected = sel;
     }
-    double *dens = density_out;
-    int32_t *sel = selected_out;
+    run_many(ctx, ests.data(), count, st);
     if (!dout) {
-      char *o = (char *)ensure(ctx, BUF_OUT, (sizeof(double) + sizeof(int32_t)) * G);
-      dens = (double *)o;
-      sel = (int32_t *)(dens + G);
-    }
-    Estimation E{p, n, d_data, d_idx, seed};
-    run_gradepro(ctx, E, dens, sel, st);
-    if (!dout) {
-      if (density_out) copy_out(density_out, dens, sizeof(double) * G, false, st);
-      if (selected_out) copy_out(selected_out, sel, sizeof(int32_t) * G, false, st);
+      for (int e = 0; e < count; ++e) {
+        const int64_t G = grid_size(&params[e].grid);
+        if (ests[e].d_density) copy_out(density_out[e], ests[e].d_density, sizeof(double) * G, false, st);
+        if (ests[e].d_selected) copy_out(selected_out[e], ests[e].d_selected, sizeof(int32_t) * G, false, st);
+      }
     }
     PKDE_CUDA_TRY(cudaStreamSynchronize(st));
     collect_trace(ctx);
   });
+}
+
+int pkde_set_step_path(pkde_ctx *ctx, int path) {
+  if (!ctx) return PKDE_EINVAL;
+  if (path != PKDE_STEPS_AUTO && path != PKDE_STEPS_PER_STEP_LAUNCH) {
+    ctx->last_error = "step path must be PKDE_STEPS_AUTO or PKDE_STEPS_PER_STEP_LAUNCH";
+    return PKDE_EINVAL;
+  }
+  ctx->step_path = path;
+  return PKDE_OK;
 }
 
 int pkde_set_profiling(pkde_ctx *ctx, int enable) {

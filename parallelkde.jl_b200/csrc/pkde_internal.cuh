@@ -80,6 +80,8 @@ enum BufId {
   BUF_TABLES,       // twiddles, propagation factors, per-step scalars
   BUF_OUT,          // device copies of outputs
   BUF_MISC,         // reductions
+  BUF_ENGINE,       // step engine: descriptors, schedule, ring slots, counters
+  BUF_BATCH,        // per-estimation buffers of a batch
   BUF_COUNT_
 };
 
@@ -94,6 +96,7 @@ struct pkde_ctx {
   size_t smem_optin = 0;
   // tracing (pkde_set_profiling / pkde_get_stats)
   bool profiling = false;
+  int step_path = 0;  // PKDE_STEPS_AUTO / PKDE_STEPS_PER_STEP_LAUNCH
   uint64_t launches = 0;
   uint64_t phase_launches[PKDE_NPHASES] = {};
   double phase_ms[PKDE_NPHASES] = {};
@@ -427,6 +430,27 @@ void copy_in(void *dst, const void *src, size_t bytes, bool src_on_device, cudaS
 void copy_out(void *dst, const void *src, size_t bytes, bool dst_on_device, cudaStream_t st);
 
 // FFT driver (pkde_fft.cu): in-place N-D transform of `batch` complex arrays.
+// Binning of one estimation into the paired spectra layout (pkde_binning.cu), in two
+// phases around one host read-back of misc[0..1] (error bits, largest count).
+struct DiracJob {
+  const pkde_grid *g = nullptr;
+  const double *d_data = nullptr;
+  int64_t n = 0;
+  const int32_t *d_idx = nullptr;
+  int64_t nboot = 0;
+  uint64_t seed = 0;
+  double2 *paired_out = nullptr;
+  uint32_t *cell = nullptr;
+  double *rh = nullptr;
+  uint32_t *counts = nullptr;
+  int *misc = nullptr;  // 256-byte device block
+  int64_t corner_off_h[16] = {};
+};
+size_t dirac_job_scratch(const pkde_grid *g, int64_t n, int64_t nboot);
+void dirac_job_bind(DiracJob &j, char *scratch, int *misc);
+void dirac_job_phase_a(pkde_ctx *ctx, DiracJob &j, cudaStream_t st);
+void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_t st);
+
 void fft_nd(pkde_ctx *ctx, int ndim, const int64_t *dims, double2 *data, int64_t batch, int dir,
             cudaStream_t st, int phase);
 // Device twiddle table for size n (cached per context).

@@ -140,6 +140,8 @@ struct EngineArgs {
 };
 bool engine_ok(const pkde_grid *g);
 void run_engine(pkde_ctx *ctx, const EngineArgs &args, cudaStream_t st);
+// Several estimations in one persistent launch (their EngineArgs are independent).
+void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStream_t st);
 
 // power-of-two path (pkde_step.cu)
 bool steps1d_ok(const pkde_grid *g);

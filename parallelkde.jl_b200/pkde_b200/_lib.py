@@ -21,9 +21,10 @@ PKDE_DEVICE_OUTPUT = 2
 # every symbol include/pkde_b200.h declares
 EXPORTED = [
     "pkde_create", "pkde_destroy", "pkde_last_error", "pkde_version",
-    "pkde_gradepro_default_params", "pkde_gradepro_estimate", "pkde_dirac_sequence",
+    "pkde_gradepro_default_params", "pkde_gradepro_estimate", "pkde_gradepro_estimate_batch", "pkde_dirac_sequence",
     "pkde_dirac_sequence_noalloc",
     "pkde_fft", "pkde_scaled_vmr", "pkde_identify_convergence", "pkde_set_profiling", "pkde_get_stats",
+    "pkde_set_step_path",
     "pkde_boot_index",
 ]
 
@@ -77,6 +78,8 @@ def load():
     lib.pkde_version.restype = ctypes.c_char_p
     lib.pkde_gradepro_default_params.argtypes = [ctypes.POINTER(PkdeGradeproParams), i32]
     lib.pkde_gradepro_estimate.argtypes = [vp, ctypes.POINTER(PkdeGradeproParams), vp, i64, vp, u64, vp, vp, u32, vp]
+    lib.pkde_gradepro_estimate_batch.argtypes = [vp, i32, ctypes.POINTER(PkdeGradeproParams), vp, vp, vp, vp, vp,
+                                                 vp, u32, vp]
     lib.pkde_dirac_sequence.argtypes = [vp, ctypes.POINTER(PkdeGrid), vp, i64, vp, i32, u64, vp, vp, vp, u32, vp]
     lib.pkde_dirac_sequence_noalloc.argtypes = [vp, ctypes.POINTER(PkdeGrid), vp, i64, vp, i32, u64, vp, vp, vp,
                                                 vp]
@@ -84,6 +87,7 @@ def load():
     lib.pkde_scaled_vmr.argtypes = [vp, i64, i32, vp, vp, i32, vp, vp, i64, vp, u32, vp]
     lib.pkde_identify_convergence.argtypes = [vp, i64, vp, vp, vp, vp, vp, dbl, dbl, i64, i64, vp, vp, vp, vp, u32, vp]
     lib.pkde_set_profiling.argtypes = [vp, ctypes.c_int]
+    lib.pkde_set_step_path.argtypes = [vp, ctypes.c_int]
     lib.pkde_get_stats.argtypes = [vp, ctypes.POINTER(PkdeStats), ctypes.c_int]
     lib.pkde_boot_index.argtypes = [u64, i64, i64, i64]
     lib.pkde_boot_index.restype = i64
@@ -151,6 +155,15 @@ def make_params(grid_struct, n_bootstraps=100, n_steps=None, bw_step=None, bw_fi
 
 def set_profiling(enable, device=0):
     load().pkde_set_profiling(context(device), int(bool(enable)))
+
+
+PKDE_STEPS_AUTO, PKDE_STEPS_PER_STEP_LAUNCH = 0, 1
+
+
+def set_step_path(path, device=0):
+    """PKDE_STEPS_AUTO (default) or PKDE_STEPS_PER_STEP_LAUNCH (the plain form)."""
+    ctx = context(device)
+    check(load().pkde_set_step_path(ctx, int(path)), ctx)
 
 
 def get_stats(device=0, reset=False):

@@ -6,7 +6,8 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (PKDE_DEVICE_INPUT, PKDE_DEVICE_OUTPUT, ArgumentError, check, context, load, make_grid_struct,
+from ._lib import (PKDE_DEVICE_INPUT, PKDE_DEVICE_OUTPUT, ArgumentError, PkdeGradeproParams, check, context, load,
+                   make_grid_struct,
                    make_params, ptr)
 
 
@@ -121,4 +122,41 @@ def gradepro_host(grid, data, density_out, selected_out=None, idx=None, seed=0, 
     p = make_params(gs, **kwargs)
     rc = lib.pkde_gradepro_estimate(ctx, ctypes.byref(p), ptr(data), int(data.shape[0]), ptr(idx),
                                     int(seed) & (2**64 - 1), ptr(density_out), ptr(selected_out), 0, stream)
+    check(rc, ctx)
+
+
+def gradepro_batch(jobs, device=False, stream=None, device_id=0):
+    """Several estimations in one pkde_gradepro_estimate_batch call.
+
+    jobs: list of dicts with keys grid, data, density, and optionally selected, idx, seed
+    and the keyword arguments of make_params (n_bootstraps, n_steps, bw_step, bw_final,
+    alpha_s, alpha_os, eps).  device=False: host NumPy arrays (data (n, N) float64
+    C-contiguous, density (G,) float64, selected (G,) int32, idx (B, n) int32);
+    device=True: CUDA torch tensors of the same shapes."""
+    lib = load()
+    ctx = context(device_id)
+    count = len(jobs)
+    params = (PkdeGradeproParams * count)()
+    keys = ("n_bootstraps", "n_steps", "bw_step", "bw_final", "alpha_s", "alpha_os", "eps")
+    vp = ctypes.c_void_p
+    data_p, idx_p, dens_p, sel_p = (vp * count)(), (vp * count)(), (vp * count)(), (vp * count)()
+    n_arr = (ctypes.c_int64 * count)()
+    seeds = (ctypes.c_uint64 * count)()
+    any_idx = any_sel = False
+    for e, j in enumerate(jobs):
+        g = j["grid"]
+        params[e] = make_params(make_grid_struct(g.lo, g.hi, g.h, g.dims), **{k: j[k] for k in keys if k in j})
+        data_p[e] = ptr(j["data"])
+        n_arr[e] = int(j["data"].shape[0])
+        dens_p[e] = ptr(j["density"])
+        seeds[e] = int(j.get("seed", 0)) & (2**64 - 1)
+        if j.get("idx") is not None:
+            idx_p[e] = ptr(j["idx"])
+            any_idx = True
+        if j.get("selected") is not None:
+            sel_p[e] = ptr(j["selected"])
+            any_sel = True
+    flags = (PKDE_DEVICE_INPUT | PKDE_DEVICE_OUTPUT) if device else 0
+    rc = lib.pkde_gradepro_estimate_batch(ctx, count, params, data_p, n_arr, idx_p if any_idx else None, seeds,
+                                          dens_p, sel_p if any_sel else None, flags, stream)
     check(rc, ctx)
