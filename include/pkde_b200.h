@@ -28,7 +28,8 @@ typedef enum pkde_status {
   PKDE_EINVAL = 1,      /* invalid argument; data beyond the grid (ArgumentError) */
   PKDE_ENOMEM = 2,      /* device allocation failed */
   PKDE_ECUDA = 3,       /* CUDA runtime error */
-  PKDE_EUNSUPPORTED = 4 /* valid request this build does not handle */
+  PKDE_EUNSUPPORTED = 4, /* valid request this build does not handle */
+  PKDE_ETIMEDOUT = 5     /* pkde_wait: the request is not done within the timeout */
 } pkde_status;
 
 /* flags for the pointer arguments */
@@ -104,6 +105,59 @@ int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradep
                                  const double *const *data, const int64_t *n, const int32_t *const *boot_idx,
                                  const uint64_t *seeds, double *const *density_out, int32_t *const *selected_out,
                                  uint32_t flags, void *stream);
+
+/* The :rot estimator (rule-of-thumb bandwidth), estimate!(::AbstractRoTEstimator, kde)
+ * on the CUDA device: RoTEstimator.jl:117-148 (initialize_estimator, initialize_density),
+ * :150-201 (estimate!, propagate_kernels!, ifft_density!), :24-49 (the rules).
+ *   rule        : PKDE_ROT_SCOTT (n^(-1/(N+4)), the reference's default) or
+ *                 PKDE_ROT_SILVERMAN ((n (N+2)/4)^(-1/(N+4))), times the per-axis
+ *                 standard deviations; the kernel is propagated by that time - h/2
+ *   data        : N x n samples (FP64);  density_out: G FP64 (|inverse FFT|)
+ * Same errors as pkde_gradepro_estimate; an unknown rule gives PKDE_EINVAL
+ * ("Rule of thumb ... not implemented."). */
+#define PKDE_ROT_SCOTT 0
+#define PKDE_ROT_SILVERMAN 1
+int pkde_rot_estimate(pkde_ctx *ctx, const pkde_grid *grid, int32_t rule, const double *data, int64_t n,
+                      double *density_out, uint32_t flags, void *stream);
+
+/* Serving: asynchronous :gradepro requests with continuous batching (no counterpart in
+ * the reference, whose estimate_density! blocks).  Submitted requests queue on the
+ * context; `lanes` worker threads, each with its own stream and device buffers, take
+ * the queued requests in arrival order as a wave (as many as fit the per-lane memory
+ * budget, at least one) and run the wave as one pkde_gradepro_estimate_batch call.
+ * While one lane's wave is on the GPU, the next arrivals start on another lane, so
+ * their work overlaps on the device.  A request's results are identical to what
+ * pkde_gradepro_estimate gives for it alone.  Inputs and outputs are host pointers
+ * owned by the caller, who keeps them valid until pkde_wait has returned the request.
+ * submit/wait are thread-safe; pkde_destroy finishes the queued requests first. */
+typedef struct pkde_request {
+  pkde_gradepro_params params;
+  const double *data;      /* N x n samples (host) */
+  int64_t n;
+  const int32_t *boot_idx; /* n x B 1-based draws (host), or NULL: seeded draws */
+  uint64_t seed;
+  double *density_out;     /* G (host) */
+  int32_t *selected_out;   /* G (host), or NULL */
+} pkde_request;
+
+typedef struct pkde_result {
+  int32_t status;          /* pkde_status of this request */
+  int32_t batch_size;      /* requests in the wave it ran in */
+  double queue_ms;         /* submit -> start of its wave */
+  double run_ms;           /* start of its wave -> done */
+  double total_ms;         /* submit -> done */
+  char message[256];       /* error message when status != PKDE_OK */
+} pkde_result;
+
+/* Lanes (1..8, default 2) and per-lane memory budget in bytes (0: 80 % of the free
+ * device memory divided by the lanes); only before the first pkde_submit. */
+int pkde_serve_config(pkde_ctx *ctx, int32_t lanes, int64_t lane_memory_bytes);
+/* Queue one request; returns its ticket.  Parameter errors are reported here (and the
+ * request is not queued); data errors (samples beyond the grid) in its result. */
+int pkde_submit(pkde_ctx *ctx, const pkde_request *req, uint64_t *ticket);
+/* Wait for a request (timeout_ms < 0: no limit).  PKDE_OK: `out` holds its result and
+ * the ticket is released; PKDE_ETIMEDOUT: not done yet; PKDE_EINVAL: unknown ticket. */
+int pkde_wait(pkde_ctx *ctx, uint64_t ticket, int32_t timeout_ms, pkde_result *out);
 
 /* Dirac-sequence binning of bootstrap resamples onto the grid.
  * Replaces initialize_dirac_sequence(Val(:cuda), ...) (DirectSpace.jl:289-362) and its

@@ -18,6 +18,9 @@ by line (citations are ``file:line`` within the reference project):
 * ladder    : src/DensityEstimators/GradeProEstimator.jl:740-796, 860-905, 954-966,
               1074-1089;  silverman_rule DirectSpace.jl:1102-1111
 * main loop : src/DensityEstimators/GradeProEstimator.jl:968-1060 (incl. replace_nans!)
+* :rot      : src/DensityEstimators/RoTEstimator.jl:24-49 (rule-of-thumb times),
+              :55-75 (time = rule - h/2), :143-148, 159-172, 177-201, 203-265
+              (identity binning, FFT, one propagation, inverse FFT, |.|)
 
 Layout: the reference is column-major with grid axis 1 fastest.  Arrays here are
 C-ordered with shape (n_N, ..., n_1) [bootstrap axis first when present], so the flat
@@ -578,6 +581,36 @@ def stable_points(ref, alt):
     noise -- typically at cells that are empty at t = 0, where the VMR is 0/0 up to
     FFT round-off -- so no implementation can reproduce it."""
     return ref.selected_step == alt.selected_step
+
+
+# ------------------------------------------------------------------------- :rot
+def rot_time(data, rule="scott"):
+    """propagation_time of the rules of thumb (RoTEstimator.jl:24-49): factor * the
+    per-axis standard deviations (diag of Statistics.cov, divisor n - 1)."""
+    data = np.asarray(data, dtype=np.float64)
+    ndim, n = data.shape
+    if rule == "silverman":
+        factor = (n * (ndim + 2) / 4) ** (-1 / (ndim + 4))
+    elif rule == "scott":
+        factor = n ** (-1 / (ndim + 4))
+    else:
+        raise ValueError(f"Rule of thumb {rule} not implemented.")
+    return factor * np.sqrt(np.var(data, axis=1, ddof=1))
+
+
+def estimate_rot(data, grid, rule="scott"):
+    """The :rot estimator on the CPU (RoTEstimator.jl:143-148, 159-201, 203-230):
+    binning of every sample once (means only), unnormalised forward FFT, propagation by
+    t = rule-of-thumb time - h/2 (RoTEstimator.jl:64-66), inverse FFT scaled by 1/G,
+    density = |.|.  Returns the density in C-order grid shape."""
+    data = np.asarray(data, dtype=np.float64)
+    n = data.shape[1]
+    ident = np.arange(1, n + 1, dtype=np.int32)[None]
+    M, _ = dirac(data, grid, ident, include_var=False)
+    Mh = fourier_statistics(M.astype(complex))[0]
+    t = rot_time(data, rule) - initial_bandwidth(grid)
+    Mt = propagate_means(Mh, grid, t)
+    return np.abs(ifourier_statistics(Mt, batched=False))
 
 
 def normalize_density(density, grid):

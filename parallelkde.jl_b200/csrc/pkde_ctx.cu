@@ -67,6 +67,7 @@ int pkde_create(pkde_ctx **out, int device) {
 int pkde_destroy(pkde_ctx *ctx) {
   if (!ctx) return PKDE_OK;
   cudaSetDevice(ctx->device);
+  pkde::stop_server(ctx);  // finishes the queued requests first
   cudaDeviceSynchronize();
   for (auto &b : ctx->buf) b.release();
   delete ctx;

@@ -351,11 +351,11 @@ Ladder make_ladder(const pkde_gradepro_params *p, const double *bw_final, int64_
   return L;
 }
 
-// Silverman's rule (DirectSpace.jl:1102-1111) from FP64 device moments, for several
-// estimations at once: two reductions, two read-backs for the whole set.
-//   data[e], n[e], N[e] -> bw[4e .. 4e+N[e]-1]
-static void silverman_batch(pkde_ctx *ctx, int count, const double *const *data, const int64_t *n, const int *N,
-                            double *bw, cudaStream_t st) {
+// Per-axis sums of squared deviations from the mean, sum_i (x_ji - mean_j)^2, of several
+// sample sets at once (FP64, deterministic): two reductions, two read-backs for the whole
+// set.  data[e] is N[e] x n[e]; the result goes to centered[4e .. 4e+N[e]-1].
+void sample_centered_sums(pkde_ctx *ctx, int count, const double *const *data, const int64_t *n, const int *N,
+                          double *centered, cudaStream_t st) {
   if (count < 1) return;
   std::vector<MomentJob> jobs(count);
   int maxnb = 1;
@@ -402,11 +402,24 @@ static void silverman_batch(pkde_ctx *ctx, int count, const double *const *data,
       PKDE_CUDA_TRY(cudaMemcpyAsync(means, h.data(), sizeof(double) * 4 * count, cudaMemcpyHostToDevice, st));
     }
   }
+  std::memcpy(centered, h.data(), sizeof(double) * 4 * count);
+}
+
+namespace {
+
+// Silverman's rule (DirectSpace.jl:1102-1111) from the FP64 device moments, for several
+// estimations at once.  data[e], n[e], N[e] -> bw[4e .. 4e+N[e]-1]
+void silverman_batch(pkde_ctx *ctx, int count, const double *const *data, const int64_t *n, const int *N, double *bw,
+                     cudaStream_t st) {
+  std::vector<double> c(4 * (size_t)std::max(count, 1));
+  sample_centered_sums(ctx, count, data, n, N, c.data(), st);
   for (int e = 0; e < count; ++e) {
     const double pref = std::pow(4.0 / ((double)(N[e] + 2) * (double)n[e]), 1.0 / (double)(N[e] + 4));
-    for (int j = 0; j < N[e]; ++j) bw[4 * e + j] = pref * std::sqrt(h[4 * e + j] / (double)(n[e] - 1));
+    for (int j = 0; j < N[e]; ++j) bw[4 * e + j] = pref * std::sqrt(c[4 * e + j] / (double)(n[e] - 1));
   }
 }
+
+}  // namespace
 
 // Per-step, per-axis propagation factors: p(k) = exp(-0.5 (k t)^2) and sqrt(p(k)),
 // k = m * (2 pi ((1/h)/n)) with fftfreq ordering (Grids.jl:225-231).
@@ -814,12 +827,82 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
   }
 }
 
-static void validate_params(const pkde_gradepro_params *p, int64_t n) {
+void validate_gradepro_params(const pkde_gradepro_params *p, int64_t n) {
   if (!p) throw invalid("params is NULL");
   grid_validate(&p->grid);
   if (p->n_bootstraps < 2) throw invalid("at least 2 bootstraps are needed (got %d)", p->n_bootstraps);
   if (p->n_steps < 0) throw invalid("n_steps must be non-negative");
   if (n < 2) throw invalid("at least 2 samples are needed");
+}
+
+// ------------------------------------------------------------------- :rot estimator
+// RoTEstimator.jl: the density is |ifft(P(k, t) * fft(dirac))| with one propagation by
+// t = rule-of-thumb time - h/2 (:64-66).  Binning of every sample once (means only,
+// :143-148 -> DirectSpace.jl:97-145), unnormalised forward FFT (:148), propagation with
+// the per-axis factors exp(-0.5 (k_j t_j)^2) applied on load of the inverse-FFT passes
+// (FourierSpace.jl:242-262 split per axis), inverse FFT scaled by 1/G (:203-230), |.|
+// (copy_density!, :233-265).
+namespace {
+__global__ void abs_kernel(int64_t G, const double2 *__restrict__ z, double *__restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < G; i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = z[i];
+    out[i] = sqrt(v.x * v.x + v.y * v.y);
+  }
+}
+}  // namespace
+
+void run_rot(pkde_ctx *ctx, const pkde_grid *g, int rule, const double *d_data, int64_t n, double *d_density,
+             cudaStream_t st) {
+  const int N = g->ndim;
+  const int64_t G = grid_size(g);
+  // propagation_time (RoTEstimator.jl:24-49): factor * sqrt(diag(cov(data))), cov with
+  // divisor n - 1
+  double c[4];
+  int Nn = N;
+  sample_centered_sums(ctx, 1, &d_data, &n, &Nn, c, st);
+  const double factor = rule == PKDE_ROT_SILVERMAN
+                            ? std::pow((double)(n * (int64_t)(N + 2)) / 4.0, -1.0 / (double)(N + 4))
+                            : std::pow((double)n, -1.0 / (double)(N + 4));
+  Ladder L{};
+  L.ndim = N;
+  L.S = 1;
+  L.times.resize(N);
+  for (int j = 0; j < N; ++j) L.times[j] = factor * std::sqrt(c[j] / (double)(n - 1)) - g->h[j] / 2;
+  std::vector<double> fz, fw;
+  std::vector<int64_t> aoff;
+  factor_tables(g, L, fz, fw, aoff);
+  const int64_t tot = aoff[N];
+  // device: [misc block][factor tables][spectrum][binning scratch]
+  const size_t off_tab = 256, off_spec = off_tab + al256(sizeof(double) * tot),
+               off_scr = off_spec + al256(sizeof(double2) * G);
+  char *base = (char *)ensure(ctx, BUF_BATCH, off_scr + dirac_job_scratch(g, n, 0));
+  double *tables = (double *)(base + off_tab);
+  double2 *spec = (double2 *)(base + off_spec);
+  PKDE_CUDA_TRY(cudaMemcpyAsync(tables, fz.data(), sizeof(double) * tot, cudaMemcpyHostToDevice, st));
+  DiracJob j;
+  j.g = g;
+  j.d_data = d_data;
+  j.n = n;
+  j.nboot = 0;
+  j.paired_out = spec;
+  dirac_job_bind(j, base + off_scr, (int *)base);
+  dirac_job_phase_a(ctx, j, st);
+  int h[64];
+  PKDE_CUDA_TRY(cudaMemcpyAsync(h, base, 256, cudaMemcpyDeviceToHost, st));
+  PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+  dirac_job_phase_b(ctx, j, h, st);
+  fft_nd(ctx, N, g->dims, spec, 1, -1, st, PKDE_PHASE_FORWARD_FFT);
+  for (int a = 0; a < N; ++a) {
+    LineSet ls = axis_lines(N, g->dims, a, 1);
+    const double *fac[1] = {tables + aoff[a]};
+    const double sc[1] = {a == 0 ? 1.0 / (double)G : 1.0};
+    fft_axis(ctx, ls, spec, spec, 1, fac, sc, 1, st, PKDE_PHASE_STEP_FFT);
+  }
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_STEP_MEANS, st);
+    abs_kernel<<<blocks_for(ctx, G), kThreads, 0, st>>>(G, spec, d_density);
+  }
+  PKDE_CHECK_LAUNCH();
 }
 
 }  // namespace pkde
@@ -846,7 +929,7 @@ int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradep
     if (count < 1 || count > 65535) throw invalid("count must be in 1..65535 (got %d)", count);
     if (!params || !data || !n) throw invalid("params, data and n are required");
     for (int e = 0; e < count; ++e) {
-      validate_params(&params[e], n[e]);
+      validate_gradepro_params(&params[e], n[e]);
       if (!data[e]) throw invalid("data[%d] is NULL", e);
     }
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
@@ -903,6 +986,34 @@ int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradep
         if (ests[e].d_selected) copy_out(selected_out[e], ests[e].d_selected, sizeof(int32_t) * G, false, st);
       }
     }
+    PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+    collect_trace(ctx);
+  });
+}
+
+int pkde_rot_estimate(pkde_ctx *ctx, const pkde_grid *grid, int32_t rule, const double *data, int64_t n,
+                      double *density_out, uint32_t flags, void *stream) {
+  return pkde_guard(ctx, [&] {
+    using namespace pkde;
+    if (!ctx) throw invalid("context is NULL");
+    grid_validate(grid);
+    if (rule != PKDE_ROT_SCOTT && rule != PKDE_ROT_SILVERMAN) throw invalid("Rule of thumb %d not implemented.", rule);
+    if (n < 2) throw invalid("at least 2 samples are needed");
+    if (!data || !density_out) throw invalid("data and density_out are required");
+    PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const int N = grid->ndim;
+    const int64_t G = grid_size(grid);
+    const bool din = flags & PKDE_DEVICE_INPUT, dout = flags & PKDE_DEVICE_OUTPUT;
+    const double *d_data = data;
+    if (!din) {
+      double *dd = (double *)ensure(ctx, BUF_DATA, sizeof(double) * N * n);
+      copy_in(dd, data, sizeof(double) * N * n, false, st);
+      d_data = dd;
+    }
+    double *dens = dout ? density_out : (double *)ensure(ctx, BUF_OUT, sizeof(double) * G);
+    run_rot(ctx, grid, rule, d_data, n, dens, st);
+    if (!dout) copy_out(density_out, dens, sizeof(double) * G, false, st);
     PKDE_CUDA_TRY(cudaStreamSynchronize(st));
     collect_trace(ctx);
   });

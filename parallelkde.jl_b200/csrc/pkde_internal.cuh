@@ -97,6 +97,10 @@ struct pkde_ctx {
   // tracing (pkde_set_profiling / pkde_get_stats)
   bool profiling = false;
   int step_path = 0;  // PKDE_STEPS_AUTO / PKDE_STEPS_PER_STEP_LAUNCH
+  // serving (pkde_serve.cu): created on the first pkde_submit
+  void *server = nullptr;
+  int serve_lanes = 2;
+  int64_t serve_lane_bytes = 0;
   uint64_t launches = 0;
   uint64_t phase_launches[PKDE_NPHASES] = {};
   double phase_ms[PKDE_NPHASES] = {};
@@ -430,6 +434,11 @@ void copy_in(void *dst, const void *src, size_t bytes, bool src_on_device, cudaS
 void copy_out(void *dst, const void *src, size_t bytes, bool dst_on_device, cudaStream_t st);
 
 // FFT driver (pkde_fft.cu): in-place N-D transform of `batch` complex arrays.
+// Argument checks of one :gradepro estimation (pkde_gradepro.cu); serving loop teardown
+// (pkde_serve.cu).
+void validate_gradepro_params(const pkde_gradepro_params *p, int64_t n);
+void stop_server(pkde_ctx *ctx);
+
 // Binning of one estimation into the paired spectra layout (pkde_binning.cu), in two
 // phases around one host read-back of misc[0..1] (error bits, largest count).
 struct DiracJob {

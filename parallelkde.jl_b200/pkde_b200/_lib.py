@@ -24,7 +24,7 @@ EXPORTED = [
     "pkde_gradepro_default_params", "pkde_gradepro_estimate", "pkde_gradepro_estimate_batch", "pkde_dirac_sequence",
     "pkde_dirac_sequence_noalloc",
     "pkde_fft", "pkde_scaled_vmr", "pkde_identify_convergence", "pkde_set_profiling", "pkde_get_stats",
-    "pkde_set_step_path",
+    "pkde_set_step_path", "pkde_rot_estimate", "pkde_serve_config", "pkde_submit", "pkde_wait",
     "pkde_boot_index",
 ]
 
@@ -88,6 +88,7 @@ def load():
     lib.pkde_identify_convergence.argtypes = [vp, i64, vp, vp, vp, vp, vp, dbl, dbl, i64, i64, vp, vp, vp, vp, u32, vp]
     lib.pkde_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.pkde_set_step_path.argtypes = [vp, ctypes.c_int]
+    lib.pkde_rot_estimate.argtypes = [vp, ctypes.POINTER(PkdeGrid), i32, vp, i64, vp, u32, vp]
     lib.pkde_get_stats.argtypes = [vp, ctypes.POINTER(PkdeStats), ctypes.c_int]
     lib.pkde_boot_index.argtypes = [u64, i64, i64, i64]
     lib.pkde_boot_index.restype = i64

@@ -259,6 +259,51 @@ class GradeProEstimator(AbstractEstimator):
 add_estimator("gradepro", GradeProEstimator)
 
 
+class RoTEstimator(AbstractEstimator):
+    """The ``:rot`` estimator (RoTEstimator.jl:107-201) on the B200 library: one
+    propagation of the binned samples by the rule-of-thumb bandwidth (``:scott``, the
+    reference's default, or ``:silverman``; RoTEstimator.jl:24-49, :117-124)."""
+
+    RULES = {"scott": 0, "silverman": 1}
+    KWARGS = ("grid", "rule_of_thumb", "stream", "device_id")
+
+    def __init__(self, grid, rule, stream, device_id):
+        self.grid = grid
+        self.rule = rule
+        self.stream = stream
+        self.device_id = device_id
+
+    @classmethod
+    def initialize_estimator(cls, kde, method="cuda", grid=None, rule_of_thumb="scott", stream=None, device_id=0,
+                             **unused):
+        for k in unused:
+            if k not in cls.KWARGS:
+                raise ArgumentError(f"unknown keyword argument {k}")
+        if grid is None:
+            raise ArgumentError("the :rot estimator needs a grid")
+        rule = str(rule_of_thumb).lstrip(":")
+        if rule not in cls.RULES:
+            raise ArgumentError(f"Rule of thumb {rule} not implemented.")
+        return cls(grid, rule, stream, device_id)
+
+    def estimate(self, kde, method="cuda", **unused):
+        ctx = context(self.device_id)
+        lib = load()
+        G = int(np.prod(self.grid.dims))
+        dens = np.empty(G, dtype=np.float64)
+        data_t = kde.samples
+        if not isinstance(data_t, np.ndarray):
+            raise ArgumentError("host samples expected; use pkde_b200.raw for device pointers")
+        gs = make_grid_struct(self.grid.lo, self.grid.hi, self.grid.h, self.grid.dims)
+        rc = lib.pkde_rot_estimate(ctx, ctypes.byref(gs), self.RULES[self.rule], ptr(data_t), data_t.shape[0],
+                                   ptr(dens), 0, self.stream)
+        check(rc, ctx)
+        kde.density[...] = dens.reshape(kde.density.shape)
+
+
+add_estimator("rot", RoTEstimator)
+
+
 def estimate_density(est, estimation_method, **kwargs):
     """estimate_density! (ParallelKDE.jl:211-226)."""
     set_nan_density(est.kde)

@@ -160,3 +160,20 @@ def gradepro_batch(jobs, device=False, stream=None, device_id=0):
     rc = lib.pkde_gradepro_estimate_batch(ctx, count, params, data_p, n_arr, idx_p if any_idx else None, seeds,
                                           dens_p, sel_p if any_sel else None, flags, stream)
     check(rc, ctx)
+
+
+def rot(grid, data, rule="scott", density=None, device=False, stream=None, device_id=0):
+    """The :rot estimator through pkde_rot_estimate.  data: (n, N) float64 C-contiguous
+    (host NumPy, or a CUDA tensor with device=True); returns the density (G,)."""
+    lib = load()
+    ctx = context(device_id)
+    rules = {"scott": 0, "silverman": 1}
+    r = rules.get(str(rule).lstrip(":"), -1)
+    gs = make_grid_struct(grid.lo, grid.hi, grid.h, grid.dims)
+    G = int(np.prod(grid.dims))
+    if density is None:
+        density = np.empty(G)
+    flags = (PKDE_DEVICE_INPUT | PKDE_DEVICE_OUTPUT) if device else 0
+    rc = lib.pkde_rot_estimate(ctx, ctypes.byref(gs), r, ptr(data), int(data.shape[0]), ptr(density), flags, stream)
+    check(rc, ctx)
+    return density

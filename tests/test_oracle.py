@@ -179,3 +179,31 @@ def test_mise_1d(oracle):
     assert _kat.mise(res.density, truth, float(grid.h[0])) < 5e-5
     assert np.all(np.isfinite(res.density))
     assert res.selected_step.min() >= 0 and res.selected_step.max() <= 251
+
+
+# ------------------------------------------------------------------------- :rot
+@pytest.mark.parametrize("n_dims", [1, 2])
+@pytest.mark.parametrize("rule", ["silverman", "scott"])
+def test_rot_mise(oracle, n_dims, rule):
+    """rulesofthumb_tests.jl:96-125: 1000 N(0, I) samples, 300 points per axis on [-6, 6],
+    MISE against the true density below 1e-3."""
+    rng = np.random.default_rng(10 + n_dims)
+    x = rng.standard_normal((n_dims, 1000))
+    grid = oracle.grid_from_ranges([(-6.0, 6.0, 300)] * n_dims)
+    d = oracle.estimate_rot(x, grid, rule)
+    axes = np.meshgrid(*([np.linspace(-6.0, 6.0, 300)] * n_dims), indexing="ij")
+    truth = np.exp(-0.5 * sum(a ** 2 for a in axes)) / (2 * np.pi) ** (n_dims / 2)
+    assert d.shape == truth.shape and not np.any(np.isnan(d))
+    assert _kat.mise(d, truth, float(np.prod(grid.h))) < 1e-3
+
+
+def test_rot_times(oracle):
+    """RoTEstimator.jl:24-49: Scott n^(-1/(N+4)), Silverman (n (N+2)/4)^(-1/(N+4)), times
+    the standard deviations (divisor n - 1)."""
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((3, 500)) * np.array([[1.0], [2.0], [0.5]])
+    sd = np.std(x, axis=1, ddof=1)
+    assert np.allclose(oracle.rot_time(x, "scott"), 500 ** (-1 / 7) * sd, rtol=1e-14)
+    assert np.allclose(oracle.rot_time(x, "silverman"), (500 * 5 / 4) ** (-1 / 7) * sd, rtol=1e-14)
+    with pytest.raises(ValueError, match="not implemented"):
+        oracle.rot_time(x, "plugin")
