@@ -164,7 +164,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "batched"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "batched", "served"])
+    ap.add_argument("--rate", type=float, default=50.0, help="requests/s (--workload served)")
+    ap.add_argument("--requests", type=int, default=64, help="requests (--workload served)")
+    ap.add_argument("--lanes", type=int, default=2, help="serving lanes (--workload served)")
     ap.add_argument("--batch", type=int, default=256, help="estimations per batch (--workload batched)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -175,6 +178,8 @@ def main():
     world, rank, local, dist = dist_setup(args)
     if args.workload == "batched":
         return run_batched(args, world, rank, local, dist)
+    if args.workload == "served":
+        return run_served(args, world, rank, local, dist)
     x, gspec, kw = workload(args.workload)
     if args.bandwidth_steps:
         kw["n_steps"] = args.bandwidth_steps
@@ -456,6 +461,82 @@ def run_batched(args, world, rank, local, dist):
                      "peak_source": peak_kind},
         "phase_ms_per_step": {p: v / args.steps for p, v in stats["phase_ms"].items()},
         "gpu_launches": stats["launches"],
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_served(args, world, rank, local, dist):
+    """--workload served: a Poisson stream of `--requests` estimations at `--rate`
+    requests/s into the serving loop (pkde_submit / pkde_wait, continuous batching over
+    `--lanes` lanes).  Latency per request (submit -> results in host memory) comes
+    from the library's timestamps; throughput = requests (and grid-point.steps) over the
+    makespan.  Host wall clock: a served stream has no single device region to time."""
+    import torch
+    import pkde_b200 as pk
+    from pkde_b200 import multi
+    from pkde_b200 import workloads as W
+    from pkde_b200.serve import Server
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pk.load()
+    pk.context(local)
+    mix = W.served_mix(count=args.requests, seed=4 + rank)
+    reqs = [(pk.find_grid(m["data"], grid_dims=m["dims"]), m) for m in mix]
+    srv = Server(device_id=local, lanes=args.lanes)
+
+    def submit(g, m, seed):
+        return srv.submit(g, m["data"], n_bootstraps=m["n_bootstraps"], n_steps=m["n_steps"], seed=seed)
+
+    for k in range(args.warmup):  # warm-up requests, one at a time
+        g, m = reqs[k % len(reqs)]
+        srv.wait(submit(g, m, 10_000 + k))
+    gaps = np.random.default_rng(7 + rank).exponential(1.0 / args.rate, len(reqs))
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    tickets = []
+    start = time.perf_counter()
+    due = start
+    for i, ((g, m), gap) in enumerate(zip(reqs, gaps)):
+        due += gap
+        delay = due - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        tickets.append(submit(g, m, i))
+    results = [srv.wait(t) for t in tickets]
+    makespan = time.perf_counter() - start
+    clk = clocks.stop()
+    bad = [r["message"] for r in results if r["status"] != 0]
+    if bad:
+        raise RuntimeError(f"served requests failed: {bad[:3]}")
+    makespan = multi.max_over_ranks(makespan, dist, dev)
+    units = sum(int(np.prod(g.dims)) * (m["n_steps"] + 1) for g, m in reqs)
+    lat = sorted(r["total_ms"] for r in results)
+    que = sorted(r["queue_ms"] for r in results)
+    pct = lambda v, q: v[min(len(v) - 1, int(q * len(v)))]
+    h2d = sum(m["data"].nbytes for _, m in reqs)
+    d2h = sum(int(np.prod(g.dims)) * 12 for g, _ in reqs)
+    kinds = {}
+    for g, _ in reqs:
+        kinds[f"{len(g.dims)}-D"] = kinds.get(f"{len(g.dims)}-D", 0) + 1
+    line = {
+        "metric": METRIC, "value": units * world / makespan, "unit": UNIT, "n_gpus": world,
+        "steps": len(reqs), "warmup": args.warmup, "ms_per_step": 1000.0 * makespan / len(reqs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"served: Poisson {args.rate:g} req/s, {len(reqs)} requests, dims 1-4, n log-uniform "
+                               "1e3-4e6, grids to 512^2 / 128^3 / 48^4, 101 bandwidths, B=32",
+                   "shapes": kinds, "lanes": args.lanes, "estimations_per_s": len(reqs) * world / makespan,
+                   "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99), "queue_p50_ms": pct(que, 0.5),
+                   "queue_p99_ms": pct(que, 0.99), "mean_wave": float(np.mean([r["batch_size"] for r in results])),
+                   "timing": "host wall clock (submit -> results in host memory)",
+                   "parallelism": f"independent request streams per rank x{world}"},
+        "e2e": {"value": units * world / makespan, "unit": UNIT, "h2d_bytes_per_step": int(h2d // len(reqs)),
+                "d2h_bytes_per_step": int(d2h // len(reqs))},
         "clocks": clk,
     }
     if rank == 0:

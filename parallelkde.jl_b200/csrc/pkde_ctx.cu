@@ -74,7 +74,7 @@ int pkde_destroy(pkde_ctx *ctx) {
   return PKDE_OK;
 }
 
-const char *pkde_last_error(const pkde_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+const char *pkde_last_error(const pkde_ctx *ctx) { return ctx ? pkde::thread_error(ctx).c_str() : "no context"; }
 
 const char *pkde_version(void) { return "pkde_b200 0.1 (sm_100a, FP64 gradepro)"; }
 

@@ -1022,7 +1022,7 @@ int pkde_rot_estimate(pkde_ctx *ctx, const pkde_grid *grid, int32_t rule, const 
 int pkde_set_step_path(pkde_ctx *ctx, int path) {
   if (!ctx) return PKDE_EINVAL;
   if (path != PKDE_STEPS_AUTO && path != PKDE_STEPS_PER_STEP_LAUNCH) {
-    ctx->last_error = "step path must be PKDE_STEPS_AUTO or PKDE_STEPS_PER_STEP_LAUNCH";
+    pkde::thread_error(ctx) = "step path must be PKDE_STEPS_AUTO or PKDE_STEPS_PER_STEP_LAUNCH";
     return PKDE_EINVAL;
   }
   ctx->step_path = path;

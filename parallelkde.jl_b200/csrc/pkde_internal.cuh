@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <map>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/pkde_b200.h"
@@ -89,7 +90,6 @@ enum BufId {
 
 struct pkde_ctx {
   int device = 0;
-  std::string last_error;
   pkde::DevBuf buf[pkde::BUF_COUNT_];
   std::map<int, pkde::DevBuf> twiddles;  // per line length
   int sm_count = 0;
@@ -176,10 +176,26 @@ __device__ __forceinline__ double2 cmul_si(double2 a, int sign) {
 // ------------------------------------------------------------------------------ FFT plan
 constexpr int kMaxStages = 24;
 
+// Division by a run-time invariant divisor d (1 <= d < 2^13) of x < 2^17 with one
+// multiply-high and a shift: q = (umulhi(x, m) + x) >> s, s = ceil(log2 d),
+// m = floor(2^32 (2^s - d) / d) + 1 (Granlund & Montgomery, "Division by invariant
+// integers using multiplication", PLDI 1994).
+struct FastDiv {
+  uint32_t m, s;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+  uint32_t s = 0;
+  while ((1u << s) < d) ++s;
+  return FastDiv{(uint32_t)(((uint64_t(1) << 32) * ((uint64_t(1) << s) - d)) / d + 1), s};
+}
+__device__ __forceinline__ uint32_t fdiv(uint32_t x, FastDiv f) { return (__umulhi(x, f.m) + x) >> f.s; }
+
 struct FftPlan {
   int n;
   int nstages;
   int radix[kMaxStages];
+  FastDiv div_nb[kMaxStages];  // per stage: n / radix
+  FastDiv div_ns[kMaxStages];  // per stage: product of the earlier radices
 };
 
 // Factor n into Stockham stages: radix 8, 4, 2 for the power-of-two part, then 3, 5,
@@ -202,6 +218,12 @@ inline FftPlan make_plan(int n) {
     }
   }
   if (m > 1) p.radix[p.nstages++] = m;
+  int ns = 1;
+  for (int st = 0; st < p.nstages; ++st) {
+    p.div_nb[st] = make_fastdiv((uint32_t)(n / p.radix[st]));
+    p.div_ns[st] = make_fastdiv((uint32_t)ns);
+    ns *= p.radix[st];
+  }
   return p;
 }
 
@@ -296,15 +318,19 @@ __device__ __forceinline__ double2 twiddle(const double2 *tw, int m, int dir) {
 
 // One Stockham stage of radix R over `nlines` lines held in shared memory
 // (line pitch `pitch` complex values).  src -> dst.
+// Lines of n < 8192 points and at most 16 lines use the plan's multiply-high divisions
+// for the butterfly indices (their range limits hold there); longer lines divide.
 template <int DIR, int R>
 __device__ __forceinline__ void stockham_stage(const double2 *src, double2 *dst, int n, int pitch,
-                                               int nlines, int Ns, const double2 *tw) {
+                                               int nlines, int Ns, const double2 *tw, FastDiv dnb, FastDiv dns) {
   const int nb = n / R;
   const int tstep = n / (Ns * R);
+  const bool fast = n < 8192 && nlines <= 16;
   for (int t = threadIdx.x; t < nlines * nb; t += blockDim.x) {
-    const int l = t / nb;
+    const int l = fast ? (int)fdiv((uint32_t)t, dnb) : t / nb;
     const int j = t - l * nb;
-    const int k = j % Ns;
+    const int jq = fast ? (int)fdiv((uint32_t)j, dns) : j / Ns;
+    const int k = j - jq * Ns;
     const double2 *s = src + l * pitch;
     double2 v[R];
 #pragma unroll
@@ -318,7 +344,7 @@ __device__ __forceinline__ void stockham_stage(const double2 *src, double2 *dst,
     if constexpr (R == 8) dft8<DIR>(v);
     if constexpr (R == 3) dft3<DIR>(v);
     if constexpr (R == 5) dft5<DIR>(v);
-    const int d = (j / Ns) * Ns * R + k;
+    const int d = jq * Ns * R + k;
     double2 *o = dst + l * pitch;
 #pragma unroll
     for (int q = 0; q < R; ++q) o[d + q * Ns] = v[q];
@@ -366,11 +392,11 @@ __device__ double2 *smem_fft(double2 *bufA, double2 *bufB, int pitch, int nlines
   for (int st = 0; st < plan.nstages; ++st) {
     const int R = plan.radix[st];
     switch (R) {
-      case 8: stockham_stage<DIR, 8>(src, dst, n, pitch, nlines, Ns, tw); break;
-      case 4: stockham_stage<DIR, 4>(src, dst, n, pitch, nlines, Ns, tw); break;
-      case 2: stockham_stage<DIR, 2>(src, dst, n, pitch, nlines, Ns, tw); break;
-      case 3: stockham_stage<DIR, 3>(src, dst, n, pitch, nlines, Ns, tw); break;
-      case 5: stockham_stage<DIR, 5>(src, dst, n, pitch, nlines, Ns, tw); break;
+      case 8: stockham_stage<DIR, 8>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
+      case 4: stockham_stage<DIR, 4>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
+      case 2: stockham_stage<DIR, 2>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
+      case 3: stockham_stage<DIR, 3>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
+      case 5: stockham_stage<DIR, 5>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
       default: stockham_stage_generic<DIR>(src, dst, n, pitch, nlines, Ns, R, tw); break;
     }
     __syncthreads();
@@ -481,17 +507,26 @@ void dirac_device(pkde_ctx *ctx, const pkde_grid *g, const double *d_data, int64
 
 }  // namespace pkde
 
-// Entry-point wrapper: converts exceptions into status codes + last_error.
+// The calling thread's last error message on a context (pkde_last_error): per thread,
+// so that threads sharing a context (pkde_submit / pkde_wait) never race on it.
+namespace pkde {
+inline std::string &thread_error(const pkde_ctx *ctx) {
+  thread_local std::unordered_map<const pkde_ctx *, std::string> errs;
+  return errs[ctx];
+}
+}  // namespace pkde
+
+// Entry-point wrapper: converts exceptions into status codes + the thread's last error.
 template <class F>
 static int pkde_guard(pkde_ctx *ctx, F &&f) {
   try {
     f();
     return PKDE_OK;
   } catch (const pkde::Error &e) {
-    if (ctx) ctx->last_error = e.msg;
+    if (ctx) pkde::thread_error(ctx) = e.msg;
     return e.code;
   } catch (const std::exception &e) {
-    if (ctx) ctx->last_error = e.what();
+    if (ctx) pkde::thread_error(ctx) = e.what();
     return PKDE_ECUDA;
   }
 }

@@ -35,6 +35,8 @@ struct Pending {
   double t_submit;
 };
 
+std::mutex g_start_mu;  // serialises the lazy start of a context's server
+
 struct Server {
   pkde_ctx *owner = nullptr;
   size_t lane_bytes = 0;
@@ -191,6 +193,7 @@ int pkde_serve_config(pkde_ctx *ctx, int32_t lanes, int64_t lane_memory_bytes) {
   return pkde_guard(ctx, [&] {
     using namespace pkde;
     if (!ctx) throw invalid("context is NULL");
+    std::lock_guard<std::mutex> lk(g_start_mu);
     if (ctx->server) throw invalid("pkde_serve_config must come before the first pkde_submit");
     if (lanes < 1 || lanes > 8) throw invalid("lanes must be in 1..8 (got %d)", lanes);
     if (lane_memory_bytes < 0) throw invalid("lane memory budget must be >= 0");
@@ -207,7 +210,10 @@ int pkde_submit(pkde_ctx *ctx, const pkde_request *req, uint64_t *ticket) {
     validate_gradepro_params(&req->params, req->n);
     if (!req->data || !req->density_out) throw invalid("data and density_out are required");
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
-    if (!ctx->server) ctx->server = start_server(ctx);
+    {
+      std::lock_guard<std::mutex> lk(g_start_mu);
+      if (!ctx->server) ctx->server = start_server(ctx);
+    }
     Server *S = (Server *)ctx->server;
     Pending p{0, *req, footprint(&req->params, req->n, req->boot_idx != nullptr), now_ms()};
     {
@@ -223,14 +229,18 @@ int pkde_submit(pkde_ctx *ctx, const pkde_request *req, uint64_t *ticket) {
 
 int pkde_wait(pkde_ctx *ctx, uint64_t ticket, int32_t timeout_ms, pkde_result *out) {
   if (!ctx || !out) return PKDE_EINVAL;
-  pkde::Server *S = (pkde::Server *)ctx->server;
+  pkde::Server *S;
+  {
+    std::lock_guard<std::mutex> lk(pkde::g_start_mu);
+    S = (pkde::Server *)ctx->server;
+  }
   if (!S) {
-    ctx->last_error = "unknown ticket";
+    pkde::thread_error(ctx) = "unknown ticket";
     return PKDE_EINVAL;
   }
   std::unique_lock<std::mutex> lk(S->mu);
   if (!S->open.count(ticket)) {
-    ctx->last_error = "unknown ticket";
+    pkde::thread_error(ctx) = "unknown ticket";
     return PKDE_EINVAL;
   }
   auto ready = [&] { return S->done.count(ticket) > 0; };

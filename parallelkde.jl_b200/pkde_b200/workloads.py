@@ -84,3 +84,27 @@ def batched_mix(count=256, seed=3, n_range=(1e3, 1e6), n_steps=100, n_boot=32):
             g = (s, s, s)
         out.append(dict(data=random_mixture(ndim, n, rng), dims=g, n_steps=n_steps, n_bootstraps=n_boot))
     return out
+
+
+def served_mix(count=48, seed=4, n_range=(1e3, 4e6), n_steps=100, n_boot=32):
+    """Served requests: dims uniform in 1..4, samples log-uniform in n_range from random
+    1-4 component Gaussian mixtures, grids 256-4096 (1-D), 128^2-512^2 (2-D), 32^3-128^3
+    (3-D), 16^4-48^4 (4-D)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        ndim = int(rng.integers(1, 5))
+        n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+        if ndim == 1:
+            g = (int(2 ** rng.integers(8, 13)),)
+        elif ndim == 2:
+            s = int(rng.choice([128, 192, 256, 320, 384, 512]))
+            g = (s, s)
+        elif ndim == 3:
+            s = int(rng.choice([32, 48, 64, 96, 128]))
+            g = (s, s, s)
+        else:
+            s = int(rng.choice([16, 24, 32, 48]))
+            g = (s, s, s, s)
+        out.append(dict(data=random_mixture(ndim, n, rng), dims=g, n_steps=n_steps, n_bootstraps=n_boot))
+    return out
