@@ -35,7 +35,18 @@ namespace pkde {
 
 namespace {
 
-constexpr int kEngineThreads = 256;
+#ifndef PKDE_ENGINE_THREADS
+#define PKDE_ENGINE_THREADS 256
+#endif
+// Threads per CTA; CTAs per SM (registers: kEngineThreads x kEngineCtas x 128 = 64K).
+constexpr int kEngineThreads = PKDE_ENGINE_THREADS;
+constexpr int kEngineCtas = 512 / kEngineThreads;
+// Lines per register tile: one butterfly per thread (the longest line of the register
+// path, 8 * kEngineThreads points, is one line per tile).
+template <int LOGN>
+constexpr int kEL = (1 << LOGN) / 8 >= kEngineThreads ? 1 : kEngineThreads * 8 / (1 << LOGN);
+template <int LOGN>
+using EP = Pow2<LOGN, kEL<LOGN>>;
 constexpr long long kSpinLimit = 20000000;  // ~1-2 s of polling, then the run aborts
 
 // One estimation's part of a launch (device-resident descriptor).
@@ -68,6 +79,7 @@ struct EngineEst {
   int gen[4];                  // 1: the axis uses the shared-memory mixed-radix FFT (any length)
   const double2 *twg[4];       // generic axes: twiddle table (cos, sin)(2 pi m / n), m < n
   FftPlan plan[4];             // generic axes: Stockham radix sequence
+  FastDiv dlen[4];             // generic axes: division by the line length
 };
 
 // A launch over one or more estimations.  Estimation e runs its local round r in global
@@ -109,7 +121,9 @@ __device__ bool wait_geq(int *error, const int *p, int target) {
   return true;
 }
 
-__host__ __device__ __forceinline__ int tile_lines_of(int logn) { return (1 << logn) / 8 > 256 ? 1 : 256 * 8 / (1 << logn); }
+__host__ __device__ __forceinline__ int tile_lines_of(int logn) {
+  return (1 << logn) / 8 >= kEngineThreads ? 1 : kEngineThreads * 8 / (1 << logn);
+}
 
 __host__ __device__ __forceinline__ int batch_arrays(const EngineEst &E, int64_t b) {
   const int j = (int)(b % (E.J + 1));
@@ -129,7 +143,7 @@ template <int LOGN>
 __device__ __forceinline__ void stage_tw(double2 *sm_tw, const double2 *tw_g, int &cached, int key) {
   if (cached != key) {  // uniform across the block
     __syncthreads();
-    for (int i = threadIdx.x; i < Pow2<LOGN>::TWSIZE; i += blockDim.x) sm_tw[i] = tw_g[i];
+    for (int i = threadIdx.x; i < EP<LOGN>::TWSIZE; i += blockDim.x) sm_tw[i] = tw_g[i];
     cached = key;
     __syncthreads();
   }
@@ -144,8 +158,8 @@ __device__ __forceinline__ void stage_tw(double2 *sm_tw, const double2 *tw_g, in
 template <int LOGN, bool FROM_SPECTRA>
 __device__ void axis_tiles(double2 *smem, const double2 *sm_tw, const double2 *in, double2 *out, int64_t inner,
                            int64_t first_tile, int ntiles, const double *f) {
-  using P = Pow2<LOGN>;
-  using I = TileIdx<LOGN, true>;
+  using P = EP<LOGN>;
+  using I = TileIdx<LOGN, true, kEL<LOGN>>;
   const int t = I::bfly();
   auto base_of = [&](int u) {
     const int64_t Lw = (first_tile + u) * P::NL + I::line();
@@ -168,7 +182,7 @@ __device__ void axis_tiles(double2 *smem, const double2 *sm_tw, const double2 *i
     for (int r = 0; r < 8; ++r) v[r] = cscale(nxt[r], f[in_pos<LOGN>(t, r)]);
     const int64_t nbase = u + 1 < ntiles ? base_of(u + 1) : base;
     if (u + 1 < ntiles) load(nbase, nxt);
-    tile_fft_reg<LOGN, 1, true>(smem, v, sm_tw);
+    tile_fft_reg<LOGN, 1, true, kEL<LOGN>>(smem, v, sm_tw);
 #pragma unroll
     for (int i = 0; i < 8; ++i) __stcg(out + base + (int64_t)out_pos<LOGN>(t, i) * inner, v[i]);
     base = nbase;
@@ -201,8 +215,8 @@ template <int LOGN>
 __device__ void vmr_tile(double2 *smem, double2 *state, double2 *sm_tw, const double2 *in, int npairs, int b0,
                          int nboot, const double *fz, const double *fw, double cz, double cw, double inv_n, int64_t G,
                          double *wst, int first, int64_t tile) {
-  using P = Pow2<LOGN>;
-  using I = TileIdx<LOGN, false>;
+  using P = EP<LOGN>;
+  using I = TileIdx<LOGN, false, kEL<LOGN>>;
   const int64_t rbase = (tile * P::NL + I::line()) * P::N;
   const int t = I::bfly();
 #pragma unroll
@@ -220,13 +234,13 @@ __device__ void vmr_tile(double2 *smem, double2 *state, double2 *sm_tw, const do
       const int k = in_pos<LOGN>(t, r);
       z[r] = cscale(__ldcg(zs + k), cz * fz[k]);
     }
-    tile_fft_reg<LOGN, 1, false>(smem, z, sm_tw);
+    tile_fft_reg<LOGN, 1, false, kEL<LOGN>>(smem, z, sm_tw);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       const int k = in_pos<LOGN>(t, r);
       w[r] = cscale(__ldcg(ws + k), cw * fw[k]);
     }
-    tile_fft_reg<LOGN, 1, false>(smem, w, sm_tw);
+    tile_fft_reg<LOGN, 1, false, kEL<LOGN>>(smem, w, sm_tw);
     const int b = b0 + 2 * p;
     const double inv_a = 1.0 / (double)(b + 1), inv_b = 1.0 / (double)(b + 2);
     const bool has_b = b + 1 < nboot;
@@ -251,8 +265,8 @@ template <int LOGN>
 __device__ void means_tile(double2 *smem, double2 *sm_tw, const double2 *in, const double *fz, double cz,
                            const double *wst, int64_t G, int nboot, double vscale, double dlogt, double eps,
                            int64_t steps_low, int64_t steps_over, const StepState &cs, int step, int64_t tile) {
-  using P = Pow2<LOGN>;
-  using I = TileIdx<LOGN, false>;
+  using P = EP<LOGN>;
+  using I = TileIdx<LOGN, false, kEL<LOGN>>;
   const int64_t rbase = (tile * P::NL + I::line()) * P::N;
   const int t = I::bfly();
   double2 z[8];
@@ -261,7 +275,7 @@ __device__ void means_tile(double2 *smem, double2 *sm_tw, const double2 *in, con
     const int k = in_pos<LOGN>(t, r);
     z[r] = cscale(__ldcg(in + rbase + k), cz * fz[k]);
   }
-  tile_fft_reg<LOGN, 1, false>(smem, z, sm_tw);
+  tile_fft_reg<LOGN, 1, false, kEL<LOGN>>(smem, z, sm_tw);
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int64_t gi = rbase + out_pos<LOGN>(t, i);
@@ -286,24 +300,22 @@ __device__ void axis_tiles_gen(double2 *smem, const double2 *in, double2 *out, i
                                const double2 *tw) {
   const int pitch = n + 1;
   double2 *bufA = smem, *bufB = smem + TL * pitch;
-  const int npts = TL * n;
+  // TL is a power of two dividing the block size: thread i always serves line i % TL,
+  // elements k = i / TL, i / TL + kstep, ...
+  const int l = threadIdx.x & (TL - 1);
+  const int kstep = blockDim.x / TL;
+  const int k0 = threadIdx.x / TL;
   for (int u = 0; u < ntiles; ++u) {
-    const int64_t L0 = (first_tile + u) * TL;
-    for (int e = threadIdx.x; e < npts; e += blockDim.x) {
-      const int k = e / TL, l = e - k * TL;
-      const int64_t L = L0 + l;
-      const int64_t off = (L / inner) * n * inner + (L % inner) + (int64_t)k * inner;
+    const int64_t L = (first_tile + u) * TL + l;
+    const int64_t base = (L / inner) * n * inner + (L % inner);
+    for (int k = k0; k < n; k += kstep) {
+      const int64_t off = base + (int64_t)k * inner;
       const double2 x = FROM_SPECTRA ? __ldcs(in + off) : __ldcg(in + off);
       bufA[l * pitch + k] = cscale(x, f[k]);
     }
     __syncthreads();
     const double2 *res = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
-    for (int e = threadIdx.x; e < npts; e += blockDim.x) {
-      const int k = e / TL, l = e - k * TL;
-      const int64_t L = L0 + l;
-      const int64_t off = (L / inner) * n * inner + (L % inner) + (int64_t)k * inner;
-      __stcg(out + off, res[l * pitch + k]);
-    }
+    for (int k = k0; k < n; k += kstep) __stcg(out + base + (int64_t)k * inner, res[l * pitch + k]);
     __syncthreads();
   }
 }
@@ -314,7 +326,7 @@ __device__ void axis_tiles_gen(double2 *smem, const double2 *in, double2 *out, i
 __device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, int npairs, int b0, int nboot,
                              const double *fz, const double *fw, double cz, double cw, double inv_n, int64_t G,
                              double *wst, int first, int64_t tile, int n1, int TL, const FftPlan &plan,
-                             const double2 *tw) {
+                             const double2 *tw, FastDiv dn1) {
   const int pitch = n1 + 1;
   double2 *bufA = smem, *bufB = smem + TL * pitch;
   const int npts = TL * n1;
@@ -326,7 +338,7 @@ __device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, i
     const double2 *ws = zs + G;
     double2 zval[8];
     for (int e = threadIdx.x; e < npts; e += blockDim.x) {
-      const int l = e / n1, k = e - l * n1;
+      const int l = (int)fdiv((uint32_t)e, dn1), k = e - l * n1;
       bufA[l * pitch + k] = cscale(__ldcg(zs + e), cz * fz[k]);
     }
     __syncthreads();
@@ -334,11 +346,11 @@ __device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, i
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const int e = threadIdx.x + q * kEngineThreads;
-      if (e < npts) zval[q] = rz[(e / n1) * pitch + (e % n1)];
+      if (e < npts) zval[q] = rz[e + (int)fdiv((uint32_t)e, dn1) * (pitch - n1)];
     }
     __syncthreads();
     for (int e = threadIdx.x; e < npts; e += blockDim.x) {
-      const int l = e / n1, k = e - l * n1;
+      const int l = (int)fdiv((uint32_t)e, dn1), k = e - l * n1;
       bufA[l * pitch + k] = cscale(__ldcg(ws + e), cw * fw[k]);
     }
     __syncthreads();
@@ -350,7 +362,7 @@ __device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, i
     for (int q = 0; q < 8; ++q) {
       const int e = threadIdx.x + q * kEngineThreads;
       if (e < npts) {
-        const double2 w = rw[(e / n1) * pitch + (e % n1)];
+        const double2 w = rw[e + (int)fdiv((uint32_t)e, dn1) * (pitch - n1)];
         double2 st = state[e];
         welford(vmr_of(zval[q].x, w.x, inv_n), inv_a, st.x, st.y);
         if (has_b) welford(vmr_of(zval[q].y, w.y, inv_n), inv_b, st.x, st.y);
@@ -369,19 +381,19 @@ __device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, i
 __device__ void means_tile_gen(double2 *smem, const double2 *in, const double *fz, double cz, const double *wst,
                                int64_t G, int nboot, double vscale, double dlogt, double eps, int64_t steps_low,
                                int64_t steps_over, const StepState &cs, int step, int64_t tile, int n1, int TL,
-                               const FftPlan &plan, const double2 *tw) {
+                               const FftPlan &plan, const double2 *tw, FastDiv dn1) {
   const int pitch = n1 + 1;
   double2 *bufA = smem, *bufB = smem + TL * pitch;
   const int npts = TL * n1;
   const int64_t rbase = tile * npts;
   for (int e = threadIdx.x; e < npts; e += blockDim.x) {
-    const int l = e / n1, k = e - l * n1;
+    const int l = (int)fdiv((uint32_t)e, dn1), k = e - l * n1;
     bufA[l * pitch + k] = cscale(__ldcg(in + rbase + e), cz * fz[k]);
   }
   __syncthreads();
   const double2 *res = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
   for (int e = threadIdx.x; e < npts; e += blockDim.x) {
-    const double2 z = res[(e / n1) * pitch + (e % n1)];
+    const double2 z = res[e + (int)fdiv((uint32_t)e, dn1) * (pitch - n1)];
     const int64_t gi = rbase + e;
     const double mu = sqrt(z.x * z.x + z.y * z.y);
     const double m2 = __ldcg(wst + G + gi);
@@ -406,7 +418,7 @@ __device__ void means_tile_gen(double2 *smem, const double2 *in, const double *f
 // GEN: some estimation of the launch has an axis on the shared-memory FFT path (a
 // separate instantiation keeps the register pressure of all-power-of-two launches low).
 template <bool GEN>
-__global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineRun R, int max_tile) {
+__global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(EngineRun R, int max_tile) {
   extern __shared__ double2 smem[];
   double2 *tile_mem = smem;
   double2 *state = smem + max_tile;
@@ -554,7 +566,7 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineRun R, 
         if (GEN && E.gen[0]) {
           vmr_tile_gen(tile_mem, state, slot_base, np, 2 * j * E.g, E.nboot, fzs + E.aoff[0], fws + E.aoff[0], E.invG,
                        E.invG * E.cw[s], E.inv_n, E.G, E.wstate + (s & 1) * 2 * E.G, j == 0, tile, (int)E.dims[0],
-                       E.tl[0], E.plan[0], E.twg[0]);
+                       E.tl[0], E.plan[0], E.twg[0], E.dlen[0]);
         } else {
           PKDE_ENGINE_SWITCH(ln, PKDE_VMR)
         }
@@ -569,7 +581,7 @@ __global__ void __launch_bounds__(kEngineThreads, 2) engine_kernel(EngineRun R, 
         if (GEN && E.gen[0]) {
           means_tile_gen(tile_mem, slot_base, fzs + E.aoff[0], E.invG, E.wstate + (s & 1) * 2 * E.G, E.G, E.nboot,
                          E.vscale[s], E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs, (int)s, tile,
-                         (int)E.dims[0], E.tl[0], E.plan[0], E.twg[0]);
+                         (int)E.dims[0], E.tl[0], E.plan[0], E.twg[0], E.dlen[0]);
         } else {
           PKDE_ENGINE_SWITCH(ln, PKDE_MEANS)
         }
@@ -596,7 +608,7 @@ int ilog2_pow2(int64_t n) {
 size_t tile_elems(int logn) {
   switch (logn) {
 #define PKDE_T(L) \
-  case L: return Pow2<L>::TILE;
+  case L: return EP<L>::TILE;
     PKDE_T(4) PKDE_T(5) PKDE_T(6) PKDE_T(7) PKDE_T(8) PKDE_T(9) PKDE_T(10) PKDE_T(11)
 #undef PKDE_T
     default: return 0;
@@ -605,7 +617,7 @@ size_t tile_elems(int logn) {
 size_t tw_elems(int logn) {
   switch (logn) {
 #define PKDE_T(L) \
-  case L: return Pow2<L>::TWSIZE;
+  case L: return EP<L>::TWSIZE;
     PKDE_T(4) PKDE_T(5) PKDE_T(6) PKDE_T(7) PKDE_T(8) PKDE_T(9) PKDE_T(10) PKDE_T(11)
 #undef PKDE_T
     default: return 0;
@@ -625,9 +637,9 @@ int engine_env_int(const char *name, int dflt, int lo, int hi) {
 }
 
 // Tile shape of grid axis j: the register radix-8 FFT where the axis is a power of two
-// in 16..2048 whose tiles line up with the layout; otherwise the shared-memory
-// mixed-radix FFT for lengths up to 2048, TL lines per tile (a power of two dividing
-// the number of lines, TL x n <= 2048).
+// in 16..8*kEngineThreads whose tiles line up with the layout; otherwise the
+// shared-memory mixed-radix FFT for lengths up to 8*kEngineThreads, TL lines per tile
+// (a power of two dividing the number of lines, TL x n <= 8*kEngineThreads).
 struct AxisShape {
   bool ok;
   int gen;
@@ -640,13 +652,13 @@ static AxisShape axis_shape(const pkde_grid *g, int j) {
   const int64_t n = g->dims[j];
   const int64_t lines = G / n;
   const int ln = ilog2_pow2(n);
-  if (ln >= 4 && ln <= 11) {
+  if (ln >= 4 && (int64_t(1) << ln) <= 8 * kEngineThreads) {
     const int nl = tile_lines_of(ln);
     if (lines % nl == 0 && (j == 0 || inner % nl == 0)) return AxisShape{true, 0, nl};
   }
-  if (n < 2 || n > 2048) return AxisShape{false, 0, 0};
+  if (n < 2 || n > 8 * kEngineThreads) return AxisShape{false, 0, 0};
   int tl = 1;
-  const int64_t cap = std::min<int64_t>(16, 2048 / n);
+  const int64_t cap = std::min<int64_t>(16, 8 * kEngineThreads / n);
   while (tl * 2 <= cap && lines % (tl * 2) == 0) tl *= 2;
   return AxisShape{true, 1, tl};
 }
@@ -732,6 +744,7 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
       if (E.gen[j]) {
         E.twg[j] = twiddles_device(ctx, (int)E.dims[j]);
         E.plan[j] = make_plan((int)E.dims[j]);
+        E.dlen[j] = make_fastdiv((uint32_t)E.dims[j]);
         max_tile = std::max(max_tile, (size_t)2 * E.tl[j] * (size_t)(E.dims[j] + 1));
       } else {
         R.tw[E.logn[j]] = stage_twiddles_device(ctx, E.logn[j]);
