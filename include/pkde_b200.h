@@ -159,6 +159,21 @@ int pkde_submit(pkde_ctx *ctx, const pkde_request *req, uint64_t *ticket);
  * the ticket is released; PKDE_ETIMEDOUT: not done yet; PKDE_EINVAL: unknown ticket. */
 int pkde_wait(pkde_ctx *ctx, uint64_t ticket, int32_t timeout_ms, pkde_result *out);
 
+/* find_grid (src/Grids/Grids.jl:252-300) from samples that may already be on the
+ * device: per-axis extrema reduced on the GPU (no copy of the samples to the host), then
+ * the reference's arithmetic: padding = 0.1 |max - min| unless given, bounds extended by
+ * the padding, n_i = dims[i] (NULL and steps NULL: 150 per axis) or, with steps,
+ * floor((hi - lo)/step) + 1 points of that step; h = (hi - lo)/(n - 1) rounded once
+ * (Julia's range(lo, stop=hi, length=n)).  data: N x n; flags PKDE_DEVICE_INPUT. */
+int pkde_find_grid(pkde_ctx *ctx, int32_t ndim, const double *data, int64_t n, const int64_t *dims,
+                   const double *steps, const double *padding, pkde_grid *out, uint32_t flags, void *stream);
+
+/* get_density(est; normalize=true) (src/ParallelKDE.jl:189-202): density /= sum(density)
+ * * dx with the sum in FP64 on the device (dx = prod(spacings(grid)), or the caller's
+ * dx).  In place; flags PKDE_DEVICE_INPUT: `density` is a device pointer.  dx <= 0 gives
+ * PKDE_EINVAL ("Normalization requires a grid or dx to be specified."). */
+int pkde_normalize_density(pkde_ctx *ctx, double *density, int64_t G, double dx, uint32_t flags, void *stream);
+
 /* Dirac-sequence binning of bootstrap resamples onto the grid.
  * Replaces initialize_dirac_sequence(Val(:cuda), ...) (DirectSpace.jl:289-362) and its
  * kernel generate_dirac_cuda! (:364-477), following the CPU arithmetic (:196-287).
@@ -224,6 +239,15 @@ int pkde_identify_convergence(pkde_ctx *ctx, int64_t G, double *density, const d
 #define PKDE_STEPS_AUTO 0
 #define PKDE_STEPS_PER_STEP_LAUNCH 1
 int pkde_set_step_path(pkde_ctx *ctx, int path);
+
+/* Autotuning of the step engine's schedule per shape (grid dimensions and bootstrap
+ * pairs): the first estimation of a new shape times trial runs over its first 16
+ * bandwidth steps for ring-slot sizes 8..64 MB, 1..8 tiles per work item and pipeline
+ * delays 2..4, and keeps the fastest for the context (and, when the environment
+ * variable PKDE_TUNE_CACHE names a file, appends it there and reads it back in later
+ * processes).  The schedule never changes results, only time.  On by default; 0 uses
+ * the fixed defaults (32 MB, 2 or 8 tiles, delay 2).  No counterpart in the reference. */
+int pkde_set_autotune(pkde_ctx *ctx, int enable);
 
 /* Launch accounting and per-phase device time, for tracing and the roofline report.
  * No counterpart in the reference, which has no tracing.

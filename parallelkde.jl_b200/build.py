@@ -13,7 +13,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = ["pkde_ctx.cu", "pkde_binning.cu", "pkde_fft.cu", "pkde_step.cu", "pkde_engine.cu", "pkde_gradepro.cu",
-       "pkde_serve.cu"]
+       "pkde_serve.cu", "pkde_grid.cu"]
 HDR = ["pkde_internal.cuh", "pkde_regfft.cuh", "pkde_step.cuh", os.path.join("..", "..", "include", "pkde_b200.h")]
 OUT = os.path.join(HERE, "lib", "libpkde_b200.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",

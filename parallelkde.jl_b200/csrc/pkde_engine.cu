@@ -26,7 +26,10 @@
 #include <cuda/atomic>
 
 #include <algorithm>
+#include <array>
+#include <cstdio>
 #include <cstring>
+#include <string>
 
 #include "pkde_regfft.cuh"
 #include "pkde_step.cuh"
@@ -696,11 +699,11 @@ EngineEst describe(const EngineArgs &A) {
   // groups mean fewer, wider batches (more independent tiles per round); measured on
   // 512 x 512 / B = 64: 74 ms at 8 MB, 58.6 ms at 16 MB, 56.9 ms at 32 MB.
   const int64_t arr_bytes = (int64_t)sizeof(double2) * E.G;
-  const int64_t slot_mb = engine_env_int("PKDE_ENGINE_SLOT_MB", 32, 1, 256);
+  const int64_t slot_mb = A.tune_slot_mb > 0 ? A.tune_slot_mb : engine_env_int("PKDE_ENGINE_SLOT_MB", 32, 1, 256);
   E.g = (int)std::max<int64_t>(1, std::min<int64_t>(E.npairs, (slot_mb << 20) / (2 * arr_bytes)));
   E.J = (E.npairs + E.g - 1) / E.g;
   // pipeline delay between passes of one batch; ring slots cover the delay
-  E.D = engine_env_int("PKDE_ENGINE_DELAY", 2, 1, 8);
+  E.D = A.tune_delay > 0 ? A.tune_delay : engine_env_int("PKDE_ENGINE_DELAY", 2, 1, 8);
   E.Q = (E.P - 1) * E.D + 2;
   E.NB = (int64_t)E.S * (E.J + 1);
   E.Tf = (int)((E.G / E.dims[0]) / E.tl[0]);
@@ -709,7 +712,7 @@ EngineEst describe(const EngineArgs &A) {
     const int64_t tiles = (E.G / E.dims[a]) / E.tl[a];
     // tiles per axis-pass item: 2 for 2-D, 8 for 3-D/4-D (measured on 128^3 / B = 32:
     // 300 ms at 2, 267 ms at 4, 246 ms at 8)
-    int want = engine_env_int("PKDE_ENGINE_TPI", E.ndim == 2 ? 2 : 8, 1, 16);
+    int want = A.tune_tpi > 0 ? A.tune_tpi : engine_env_int("PKDE_ENGINE_TPI", E.ndim == 2 ? 2 : 8, 1, 16);
     while (want > 1 && tiles % want) want >>= 1;
     E.tpi[a] = want;
   }
@@ -894,5 +897,87 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
 }
 
 void run_engine(pkde_ctx *ctx, const EngineArgs &A, cudaStream_t st) { run_engine_batch(ctx, &A, 1, st); }
+
+// ---------------------------------------------------------------- autotuning
+// Key of a shape: grid dimensions and pairs of bootstraps (the schedule depends on
+// nothing else).
+static std::string tune_key(const EngineArgs &A) {
+  std::string k = std::to_string(A.grid->ndim);
+  for (int j = 0; j < A.grid->ndim; ++j) k += "x" + std::to_string(A.grid->dims[j]);
+  return k + ":p" + std::to_string(A.npairs);
+}
+
+static void load_tune_file(pkde_ctx *ctx) {
+  if (ctx->tune_loaded) return;
+  ctx->tune_loaded = true;
+  const char *path = getenv("PKDE_TUNE_CACHE");
+  if (!path || !*path) return;
+  FILE *f = fopen(path, "r");
+  if (!f) return;
+  char key[256];
+  int a, b, c;
+  while (fscanf(f, "%255s %d %d %d", key, &a, &b, &c) == 4) ctx->tune[key] = {a, b, c};
+  fclose(f);
+}
+
+static void save_tune(pkde_ctx *ctx, const std::string &key, const std::array<int, 3> &v) {
+  const char *path = getenv("PKDE_TUNE_CACHE");
+  if (!path || !*path) return;
+  FILE *f = fopen(path, "a");
+  if (!f) return;
+  fprintf(f, "%s %d %d %d\n", key.c_str(), v[0], v[1], v[2]);
+  fclose(f);
+}
+
+void autotune_engine(pkde_ctx *ctx, EngineArgs &A, cudaStream_t st) {
+  load_tune_file(ctx);
+  const std::string key = tune_key(A);
+  auto it = ctx->tune.find(key);
+  if (it == ctx->tune.end()) {
+    if (!ctx->autotune) return;
+    // trial runs over the first bandwidth steps of this estimation
+    EngineArgs T = A;
+    T.S = std::min(A.S, 16);
+    const bool twoD = A.grid->ndim == 2;
+    std::vector<std::array<int, 3>> cand;
+    for (int slot : {8, 16, 32, 64})
+      for (int tpi : {1, 2, 4, 8}) cand.push_back({slot, tpi, 2});
+    cudaEvent_t e0, e1;
+    PKDE_CUDA_TRY(cudaEventCreate(&e0));
+    PKDE_CUDA_TRY(cudaEventCreate(&e1));
+    auto trial = [&](const std::array<int, 3> &c) {
+      T.tune_slot_mb = c[0];
+      T.tune_tpi = c[1];
+      T.tune_delay = c[2];
+      run_engine_batch(ctx, &T, 1, st);  // warm (buffers sized, code loaded)
+      PKDE_CUDA_TRY(cudaEventRecord(e0, st));
+      run_engine_batch(ctx, &T, 1, st);
+      PKDE_CUDA_TRY(cudaEventRecord(e1, st));
+      PKDE_CUDA_TRY(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      PKDE_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+      return ms;
+    };
+    std::array<int, 3> best = {32, twoD ? 2 : 8, 2};
+    float best_ms = trial(best);
+    for (const auto &c : cand) {
+      const float ms = trial(c);
+      if (ms < best_ms) best_ms = ms, best = c;
+    }
+    for (int d : {3, 4}) {
+      std::array<int, 3> c = best;
+      c[2] = d;
+      const float ms = trial(c);
+      if (ms < best_ms) best_ms = ms, best = c;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    it = ctx->tune.emplace(key, best).first;
+    save_tune(ctx, key, best);
+  }
+  A.tune_slot_mb = it->second[0];
+  A.tune_tpi = it->second[1];
+  A.tune_delay = it->second[2];
+}
 
 }  // namespace pkde

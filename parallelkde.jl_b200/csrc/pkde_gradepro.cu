@@ -779,16 +779,19 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
       converge_steps(ctx, P.G, (int)S, f_all, mu_all, d_dl, L.eps, L.steps_low, L.steps_over, P.cs, st);
       continue;
     }
-    {
-      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-      init_state_kernel<<<blocks_for(ctx, P.G), kThreads, 0, st>>>(P.G, P.cs);
-    }
-    PKDE_CHECK_LAUNCH();
+    auto init_state = [&] {
+      {
+        ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+        init_state_kernel<<<blocks_for(ctx, P.G), kThreads, 0, st>>>(P.G, P.cs);
+      }
+      PKDE_CHECK_LAUNCH();
+    };
     if (P.path == StepPath::Generic) {
+      init_state();
       run_generic(ctx, P, st);
       continue;
     }
-    // N-D on power-of-two axes: the persistent step engine
+    // N-D: the persistent step engine, schedule parameters per shape (autotuned once)
     EngineArgs A{};
     A.grid = P.g;
     A.npairs = (int)P.npairs;
@@ -807,6 +810,8 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
     A.steps_low = L.steps_low;
     A.steps_over = L.steps_over;
     A.cs = P.cs;
+    autotune_engine(ctx, A, st);  // trial runs (if any) overwrite the state: initialise after
+    init_state();
     eng.push_back(A);
     eng_who.push_back(e);
   }
@@ -1026,6 +1031,12 @@ int pkde_set_step_path(pkde_ctx *ctx, int path) {
     return PKDE_EINVAL;
   }
   ctx->step_path = path;
+  return PKDE_OK;
+}
+
+int pkde_set_autotune(pkde_ctx *ctx, int enable) {
+  if (!ctx) return PKDE_EINVAL;
+  ctx->autotune = enable != 0;
   return PKDE_OK;
 }
 

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <array>
 #include <map>
 #include <string>
 #include <unordered_map>
@@ -97,6 +98,10 @@ struct pkde_ctx {
   // tracing (pkde_set_profiling / pkde_get_stats)
   bool profiling = false;
   int step_path = 0;  // PKDE_STEPS_AUTO / PKDE_STEPS_PER_STEP_LAUNCH
+  // engine schedule per shape (pkde_set_autotune): key -> {slot MB, tiles per item, delay}
+  bool autotune = true;
+  bool tune_loaded = false;
+  std::map<std::string, std::array<int, 3>> tune;
   // serving (pkde_serve.cu): created on the first pkde_submit
   void *server = nullptr;
   int serve_lanes = 2;

@@ -137,8 +137,15 @@ struct EngineArgs {
   double inv_n, eps;
   int64_t steps_low, steps_over;
   StepState cs;
+  // schedule parameters (0: default): ring-slot MB, tiles per axis-pass item, pipeline
+  // delay between the passes of a batch
+  int tune_slot_mb = 0, tune_tpi = 0, tune_delay = 0;
 };
 bool engine_ok(const pkde_grid *g);
+// Per-shape schedule parameters: from the context's cache, else (autotuning on) timed
+// trial runs of the estimation's first bandwidth steps.  Overwrites the estimation's
+// convergence state (the caller initialises it afterwards).
+void autotune_engine(pkde_ctx *ctx, EngineArgs &args, cudaStream_t st);
 void run_engine(pkde_ctx *ctx, const EngineArgs &args, cudaStream_t st);
 // Several estimations in one persistent launch (their EngineArgs are independent).
 void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStream_t st);

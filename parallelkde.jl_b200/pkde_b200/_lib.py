@@ -25,6 +25,7 @@ EXPORTED = [
     "pkde_dirac_sequence_noalloc",
     "pkde_fft", "pkde_scaled_vmr", "pkde_identify_convergence", "pkde_set_profiling", "pkde_get_stats",
     "pkde_set_step_path", "pkde_rot_estimate", "pkde_serve_config", "pkde_submit", "pkde_wait",
+    "pkde_find_grid", "pkde_normalize_density", "pkde_set_autotune",
     "pkde_boot_index",
 ]
 
@@ -88,6 +89,9 @@ def load():
     lib.pkde_identify_convergence.argtypes = [vp, i64, vp, vp, vp, vp, vp, dbl, dbl, i64, i64, vp, vp, vp, vp, u32, vp]
     lib.pkde_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.pkde_set_step_path.argtypes = [vp, ctypes.c_int]
+    lib.pkde_set_autotune.argtypes = [vp, ctypes.c_int]
+    lib.pkde_find_grid.argtypes = [vp, i32, vp, i64, vp, vp, vp, ctypes.POINTER(PkdeGrid), u32, vp]
+    lib.pkde_normalize_density.argtypes = [vp, vp, i64, dbl, u32, vp]
     lib.pkde_rot_estimate.argtypes = [vp, ctypes.POINTER(PkdeGrid), i32, vp, i64, vp, u32, vp]
     lib.pkde_get_stats.argtypes = [vp, ctypes.POINTER(PkdeStats), ctypes.c_int]
     lib.pkde_boot_index.argtypes = [u64, i64, i64, i64]
@@ -165,6 +169,12 @@ def set_step_path(path, device=0):
     """PKDE_STEPS_AUTO (default) or PKDE_STEPS_PER_STEP_LAUNCH (the plain form)."""
     ctx = context(device)
     check(load().pkde_set_step_path(ctx, int(path)), ctx)
+
+
+def set_autotune(enable, device=0):
+    """Per-shape autotuning of the step engine's schedule (on by default)."""
+    ctx = context(device)
+    check(load().pkde_set_autotune(ctx, int(bool(enable))), ctx)
 
 
 def get_stats(device=0, reset=False):

@@ -37,7 +37,10 @@ class KDE:
 
     def __init__(self, data, dims):
         self.data = data
-        self.samples = np.ascontiguousarray(np.asarray(data).T)
+        if hasattr(data, "is_cuda"):  # samples already on the GPU stay there
+            self.samples = data.double().t().contiguous()
+        else:
+            self.samples = np.ascontiguousarray(np.asarray(data).T)
         self.density = np.full(tuple(reversed(dims)), np.nan)
         self.dims = tuple(dims)
         self._pinned = None
@@ -48,6 +51,8 @@ class KDE:
 
     def pin(self):
         """Keep the samples in page-locked host memory (faster host-to-device copies)."""
+        if not isinstance(self.samples, np.ndarray):
+            return self
         import torch
         t = torch.empty(self.samples.shape, dtype=torch.float64, pin_memory=True)
         t.numpy()[...] = self.samples
@@ -134,10 +139,14 @@ def initialize_estimation(data, grid=False, grid_ranges=None, dims=None, grid_bo
         if grid:
             if grid_ranges is not None:
                 grid = initialize_grid(grid_ranges, device=device)
-            else:
+            elif isinstance(a, np.ndarray) or grid_bounds is not None:
                 host = a if isinstance(a, np.ndarray) else a.double().cpu().numpy()
                 grid = find_grid(host, grid_bounds=grid_bounds, grid_dims=dims, grid_padding=grid_padding,
                                  device=device)
+            else:  # samples already on the GPU: extrema reduced there (pkde_find_grid)
+                from . import raw
+                grid = raw.find_grid_device(a.double().t().contiguous(), grid_dims=dims, grid_padding=grid_padding,
+                                            device=True, device_id=a.device.index or 0)
         else:
             grid = None
     elif getattr(grid, "device", device) != device:
@@ -158,12 +167,14 @@ def get_grid(est):
 
 
 def get_density(est, normalize=False, dx=None):
-    """ParallelKDE.jl:189-202 (normalisation sum in FP64)."""
+    """ParallelKDE.jl:189-202: with normalize, density /= sum(density) * prod(spacings)
+    (or dx), the sum in FP64 on the GPU (pkde_normalize_density)."""
+    from . import raw
     d = est.kde.density
     if normalize and has_grid(est):
-        d /= np.sum(d, dtype=np.float64) * float(np.prod(est.grid.h))
+        raw.normalize_density(np.ascontiguousarray(d) if not d.flags.c_contiguous else d, float(np.prod(est.grid.h)))
     elif normalize and dx is not None:
-        d /= np.sum(d, dtype=np.float64) * dx
+        raw.normalize_density(d, float(dx))
     elif normalize:
         raise ArgumentError("Normalization requires a grid or dx to be specified.")
     return d
@@ -246,10 +257,14 @@ class GradeProEstimator(AbstractEstimator):
         dens = np.empty(G, dtype=np.float64)
         sel = np.empty(G, dtype=np.int32)
         data_t = kde.samples  # (n, N) C-contiguous == N x n column-major
-        if not isinstance(data_t, np.ndarray):
-            raise ArgumentError("host samples expected; use pkde_b200.raw for device pointers")
+        flags, idx = 0, self.idx
+        if not isinstance(data_t, np.ndarray):  # device samples: device inputs, host outputs
+            flags = _lib.PKDE_DEVICE_INPUT
+            if idx is not None:
+                import torch
+                idx = torch.from_numpy(idx).to(data_t.device)
         rc = lib.pkde_gradepro_estimate(ctx, ctypes.byref(self.params), ptr(data_t), data_t.shape[0],
-                                        ptr(self.idx), int(self.seed) & (2**64 - 1), ptr(dens), ptr(sel), 0,
+                                        ptr(idx), int(self.seed) & (2**64 - 1), ptr(dens), ptr(sel), flags,
                                         self.stream)
         check(rc, ctx)
         kde.density[...] = dens.reshape(kde.density.shape)
@@ -292,11 +307,10 @@ class RoTEstimator(AbstractEstimator):
         G = int(np.prod(self.grid.dims))
         dens = np.empty(G, dtype=np.float64)
         data_t = kde.samples
-        if not isinstance(data_t, np.ndarray):
-            raise ArgumentError("host samples expected; use pkde_b200.raw for device pointers")
+        flags = 0 if isinstance(data_t, np.ndarray) else _lib.PKDE_DEVICE_INPUT
         gs = make_grid_struct(self.grid.lo, self.grid.hi, self.grid.h, self.grid.dims)
         rc = lib.pkde_rot_estimate(ctx, ctypes.byref(gs), self.RULES[self.rule], ptr(data_t), data_t.shape[0],
-                                   ptr(dens), 0, self.stream)
+                                   ptr(dens), flags, self.stream)
         check(rc, ctx)
         kde.density[...] = dens.reshape(kde.density.shape)
 

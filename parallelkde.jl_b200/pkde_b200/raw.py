@@ -177,3 +177,33 @@ def rot(grid, data, rule="scott", density=None, device=False, stream=None, devic
     rc = lib.pkde_rot_estimate(ctx, ctypes.byref(gs), r, ptr(data), int(data.shape[0]), ptr(density), flags, stream)
     check(rc, ctx)
     return density
+
+
+def find_grid_device(data, grid_dims=None, grid_steps=None, grid_padding=None, device=False, stream=None,
+                     device_id=0):
+    """find_grid (Grids.jl:252-300) with the extrema reduced on the GPU: data (n, N)
+    float64 C-contiguous host array, or a CUDA tensor with device=True.  Returns a Grid."""
+    from .grids import Grid
+    from ._lib import PkdeGrid
+    lib = load()
+    ctx = context(device_id)
+    n, N = int(data.shape[0]), int(data.shape[1])
+    dims = None if grid_dims is None else np.ascontiguousarray(grid_dims, dtype=np.int64)
+    steps = None if grid_steps is None else np.ascontiguousarray(grid_steps, dtype=np.float64)
+    pad = None if grid_padding is None else np.ascontiguousarray(grid_padding, dtype=np.float64)
+    g = PkdeGrid()
+    rc = lib.pkde_find_grid(ctx, N, ptr(data), n, ptr(dims), ptr(steps), ptr(pad), ctypes.byref(g),
+                            PKDE_DEVICE_INPUT if device else 0, stream)
+    check(rc, ctx)
+    return Grid([g.lo[j] for j in range(N)], [g.hi[j] for j in range(N)], [g.dims[j] for j in range(N)],
+                [g.h[j] for j in range(N)])
+
+
+def normalize_density(density, dx, device=False, stream=None, device_id=0):
+    """density /= sum(density) * dx in place, FP64 sum on the GPU (ParallelKDE.jl:189-202)."""
+    lib = load()
+    ctx = context(device_id)
+    G = int(np.prod(density.shape))
+    rc = lib.pkde_normalize_density(ctx, ptr(density), G, float(dx), PKDE_DEVICE_INPUT if device else 0, stream)
+    check(rc, ctx)
+    return density

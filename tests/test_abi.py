@@ -97,9 +97,23 @@ def test_find_grid_and_normalisation():
     assert np.allclose(g.initial_bandwidth(), g.spacings() / 2)
     k = g.fftgrid()
     assert np.allclose(k[0], 2 * np.pi * np.fft.fftfreq(11, 2.4 / 10))
-    est = pk.initialize_estimation(data, grid=g)
-    est.kde.density[...] = 1.0
-    d = pk.get_density(est, normalize=True)
-    assert np.isclose(d.sum() * np.prod(g.spacings()), 1.0)
+    # normalisation runs on the GPU (tests/test_gpu_grid.py); without a grid or dx it
+    # is an ArgumentError before any device work (ParallelKDE.jl:198-199)
+    est = pk.initialize_estimation(data, dims=(11, 21))
+    with pytest.raises(pk.ArgumentError, match="Normalization requires"):
+        pk.get_density(est, normalize=True)
     gg = pk.initialize_grid([np.linspace(-5, 5, 101)])
     assert gg.dims == (101,) and np.isclose(gg.h[0], 0.1)
+
+
+def test_parallelkdepy_surface_grid():
+    """The ParallelKDEpy Grid of the reference's benchmark notebook: shape in axis order,
+    meshgrid with indexing "ij"."""
+    import pkde_b200.parallelkdepy as pkdepy
+    g = pkdepy.Grid(2 * [(-8.0, 8.0, 33)] + [(-1.0, 1.0, 5)], device="cuda")
+    assert g.shape == (33, 33, 5)
+    m = g.to_meshgrid()
+    assert len(m) == 3 and m[0].shape == (33, 33, 5)
+    assert m[0][4, 0, 0] == -8.0 + 4 * 0.5 and m[2][0, 0, 4] == 1.0
+    with pytest.raises(pkdepy.ArgumentError):
+        pkdepy.Grid([(-1.0, 1.0, 5)], device="cpu")

@@ -152,3 +152,33 @@ def test_plain_form_agrees_with_engine(pk, dims, n, B, steps):
     assert same.mean() >= 0.99
     rel = np.linalg.norm((d_auto - d_plain)[same]) / np.linalg.norm(d_plain[same])
     assert rel <= 1e-10, rel
+
+
+def test_autotune_keeps_results_and_caches(pk, tmp_path, monkeypatch):
+    """The per-shape schedule search changes time only: results with autotuning on and
+    off are identical; the chosen schedule is appended to PKDE_TUNE_CACHE."""
+    import ctypes
+    from pkde_b200 import _lib
+    lib = _lib.load()
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("PKDE_TUNE_CACHE", str(cache))
+    rng = np.random.default_rng(12)
+    x = rng.standard_normal((2, 6000))
+    grid = pk.find_grid(x, grid_dims=(64, 48))
+    p = _lib.make_params(_lib.make_grid_struct(grid.lo, grid.hi, grid.h, grid.dims), 10, 20)
+    data = np.ascontiguousarray(x.T)
+    outs = []
+    for tune in (0, 1):
+        ctx = ctypes.c_void_p()
+        assert lib.pkde_create(ctypes.byref(ctx), 0) == 0
+        assert lib.pkde_set_autotune(ctx, tune) == 0
+        d = np.empty(grid.dims[0] * grid.dims[1])
+        s = np.empty(d.size, dtype=np.int32)
+        rc = lib.pkde_gradepro_estimate(ctx, ctypes.byref(p), _lib.ptr(data), data.shape[0], None, 3, _lib.ptr(d),
+                                        _lib.ptr(s), 0, None)
+        assert rc == 0
+        outs.append((d, s))
+        lib.pkde_destroy(ctx)
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    lines = cache.read_text().split()
+    assert lines and lines[0] == "2x64x48:p5" and len(lines) == 4

@@ -61,3 +61,21 @@ def test_rot_errors_and_device_pointers(pk, oracle):
     raw.rot(grid, dd, "scott", density=out, device=True, stream=torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), host)
+
+
+def test_parallelkdepy_surface_estimates(pk):
+    """paper/benchmark_time.ipynb's ParallelKDE class: Grid, DensityEstimation(data n x
+    dim), estimate_density(method), get_density() -- same numbers as the main API."""
+    import pkde_b200.parallelkdepy as pkdepy
+    rng = np.random.default_rng(5)
+    data = rng.standard_normal((3000, 2))
+    grid = pkdepy.Grid(2 * [(-8.0, 8.0, 64)], device="cuda")
+    for method in ("gradepro", ":rot"):
+        est = pkdepy.DensityEstimation(data, grid=grid, device="cuda")
+        kw = dict(n_bootstraps=8, n_steps=20) if method == "gradepro" else {}
+        est.estimate_density(method, **kw)
+        d = est.get_density()
+        assert d.shape == grid.shape
+        ref = pk.initialize_estimation(data.T, grid=True, grid_ranges=2 * [(-8.0, 8.0, 64)], device="cuda")
+        pk.estimate_density(ref, method.lstrip(":"), **kw)
+        assert np.array_equal(d, pk.get_density(ref).T)
