@@ -159,8 +159,8 @@ __device__ __forceinline__ void stage_tw(double2 *sm_tw, const double2 *tw_g, in
 // not push the ring slots out of L2; otherwise the input is a ring slot written by
 // other CTAs and is read through L2 only.
 template <int LOGN, bool FROM_SPECTRA>
-__device__ void axis_tiles(double2 *smem, const double2 *sm_tw, const double2 *in, double2 *out, int64_t inner,
-                           int64_t first_tile, int ntiles, const double *f) {
+__device__ void axis_tiles(double2 *smem, double2 *smem2, const double2 *sm_tw, const double2 *in, double2 *out,
+                           int64_t inner, int64_t first_tile, int ntiles, const double *f) {
   using P = EP<LOGN>;
   using I = TileIdx<LOGN, true, kEL<LOGN>>;
   const int t = I::bfly();
@@ -185,7 +185,7 @@ __device__ void axis_tiles(double2 *smem, const double2 *sm_tw, const double2 *i
     for (int r = 0; r < 8; ++r) v[r] = cscale(nxt[r], f[in_pos<LOGN>(t, r)]);
     const int64_t nbase = u + 1 < ntiles ? base_of(u + 1) : base;
     if (u + 1 < ntiles) load(nbase, nxt);
-    tile_fft_reg<LOGN, 1, true, kEL<LOGN>>(smem, v, sm_tw);
+    tile_fft_reg<LOGN, 1, true, kEL<LOGN>, true>(smem, v, sm_tw, smem2);
 #pragma unroll
     for (int i = 0; i < 8; ++i) __stcg(out + base + (int64_t)out_pos<LOGN>(t, i) * inner, v[i]);
     base = nbase;
@@ -421,11 +421,14 @@ __device__ void means_tile_gen(double2 *smem, const double2 *in, const double *f
 // GEN: some estimation of the launch has an axis on the shared-memory FFT path (a
 // separate instantiation keeps the register pressure of all-power-of-two launches low).
 template <bool GEN>
-__global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(EngineRun R, int max_tile) {
+__global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(EngineRun R, int max_tile,
+                                                                             int state_elems) {
   extern __shared__ double2 smem[];
+  // [tile][state: Welford state of the final pass, second exchange buffer of the axis
+  // passes][twiddles]
   double2 *tile_mem = smem;
   double2 *state = smem + max_tile;
-  double2 *sm_tw = state + 8 * kEngineThreads;
+  double2 *sm_tw = state + state_elems;
   __shared__ EngineEst sE;  // descriptor of the estimation the current item belongs to
   __shared__ int64_t s_next, s_b, s_tile, s_round, s_off;
   __shared__ int s_p, s_ok, s_e;
@@ -540,9 +543,9 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
   {                                                                                       \
     stage_tw<L>(sm_tw, R.tw[L], cached_tw, L);                                            \
     if (p == 0)                                                                           \
-      axis_tiles<L, true>(tile_mem, sm_tw, in, out, inner, first_tile, tpi, f);           \
+      axis_tiles<L, true>(tile_mem, state, sm_tw, in, out, inner, first_tile, tpi, f);    \
     else                                                                                  \
-      axis_tiles<L, false>(tile_mem, sm_tw, in, out, inner, first_tile, tpi, f);          \
+      axis_tiles<L, false>(tile_mem, state, sm_tw, in, out, inner, first_tile, tpi, f);   \
   }
       if (GEN && E.gen[a]) {
         if (p == 0)
@@ -737,7 +740,7 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
   if (count < 1) return;
   std::vector<EngineEst> est(count);
   std::vector<std::vector<int64_t>> rs(count);
-  size_t max_tile = 0, max_tw = 1;
+  size_t max_tile = 0, max_tw = 1, max_reg_tile = 0;
   EngineRun R{};
   for (int l = 0; l < 13; ++l) R.tw[l] = nullptr;
   for (int e = 0; e < count; ++e) {
@@ -752,6 +755,7 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
       } else {
         R.tw[E.logn[j]] = stage_twiddles_device(ctx, E.logn[j]);
         max_tile = std::max(max_tile, tile_elems(E.logn[j]));
+        max_reg_tile = std::max(max_reg_tile, tile_elems(E.logn[j]));
         max_tw = std::max(max_tw, tw_elems(E.logn[j]));
       }
     }
@@ -879,7 +883,9 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
   for (int e = 0; e < count; ++e)
     for (int j = 0; j < est[e].ndim; ++j) any_gen |= est[e].gen[j] != 0;
   auto kern = any_gen ? engine_kernel<true> : engine_kernel<false>;
-  const size_t smem = sizeof(double2) * (max_tile + 8 * kEngineThreads + max_tw);
+  // the state region doubles as the second exchange buffer of the register-FFT axis passes
+  const size_t state_elems = std::max<size_t>(max_reg_tile, 8 * kEngineThreads);
+  const size_t smem = sizeof(double2) * (max_tile + state_elems + max_tw);
   PKDE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   PKDE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEngineThreads, smem));
@@ -887,7 +893,7 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
   const int64_t grid = std::min<int64_t>(total, (int64_t)per_sm * ctx->sm_count);
   if (grid > 0) {
     Trace tr(ctx, PKDE_PHASE_STEP_VMR, st);
-    kern<<<(unsigned)grid, kEngineThreads, smem, st>>>(R, (int)max_tile);
+    kern<<<(unsigned)grid, kEngineThreads, smem, st>>>(R, (int)max_tile, (int)state_elems);
   }
   PKDE_CHECK_LAUNCH();
   int err = 0;

@@ -191,39 +191,48 @@ __device__ __forceinline__ void tail2(double2 *line, double2 *v, int t, const do
   }
 }
 
-template <int LOGN, int DIR, int ST, bool COLS, int NLINES>
-__device__ __forceinline__ void run_stages(double2 *line, double2 *v, int t, const double2 *tw, int l) {
+// DB (double buffering): exchange k (the store of stage k) goes to buffer k % 2, so the
+// barrier after each load is not needed: the next store goes to the other buffer, and
+// the store after that follows another barrier that every thread reaches only after its
+// loads.  The tile is free for the next call when the last exchange used buffer 1; after
+// an exchange through buffer 0 a trailing barrier keeps that guarantee.
+template <int LOGN, int DIR, int ST, bool COLS, int NLINES, bool DB = false>
+__device__ __forceinline__ void run_stages(double2 *line, double2 *line2, double2 *v, int t, const double2 *tw,
+                                           int l) {
   using P = Pow2<LOGN>;
   stage8_compute<LOGN, DIR, ST>(v, t, tw);
   constexpr bool last8 = ST + 1 == P::NST8;
+  double2 *buf = (DB && (ST & 1)) ? line2 : line;
   if constexpr (last8 && P::REM == 0) {
+    if constexpr (DB && ST >= 1 && ((ST - 1) & 1) == 0) line_sync<LOGN, COLS, NLINES>(l);
     return;  // outputs stay in registers: v[q] = X[t + q*N/8]
   } else {
-    stage8_store<LOGN, ST>(line, v, t);
+    stage8_store<LOGN, ST>(buf, v, t);
     line_sync<LOGN, COLS, NLINES>(l);
     if constexpr (!last8) {
-      load8<LOGN>(line, v, t);
-      line_sync<LOGN, COLS, NLINES>(l);
-      run_stages<LOGN, DIR, ST + 1, COLS, NLINES>(line, v, t, tw, l);
+      load8<LOGN>(buf, v, t);
+      if constexpr (!DB) line_sync<LOGN, COLS, NLINES>(l);
+      run_stages<LOGN, DIR, ST + 1, COLS, NLINES, DB>(line, line2, v, t, tw, l);
     } else if constexpr (P::REM == 2) {
-      tail4<LOGN, DIR>(line, v, t, tw);
-      line_sync<LOGN, COLS, NLINES>(l);
+      tail4<LOGN, DIR>(buf, v, t, tw);
+      if constexpr (!DB || (ST & 1) == 0) line_sync<LOGN, COLS, NLINES>(l);
     } else {
-      tail2<LOGN, DIR>(line, v, t, tw);
-      line_sync<LOGN, COLS, NLINES>(l);
+      tail2<LOGN, DIR>(buf, v, t, tw);
+      if constexpr (!DB || (ST & 1) == 0) line_sync<LOGN, COLS, NLINES>(l);
     }
   }
 }
 
 // FFT of the thread's line.  On entry v[r] = x[in_pos(t, r)]; on exit v[i] =
 // X[out_pos(t, i)].  Every thread of the line (COLS: of the block) must call it; the
-// line's tile memory is free again when it returns.
-template <int LOGN, int DIR, bool COLS, int NLINES = 0>
-__device__ __forceinline__ void tile_fft_reg(double2 *tile, double2 *v, const double2 *tw) {
+// line's tile memory (and tile2 with DB) is free again for the next call when it returns.
+template <int LOGN, int DIR, bool COLS, int NLINES = 0, bool DB = false>
+__device__ __forceinline__ void tile_fft_reg(double2 *tile, double2 *v, const double2 *tw, double2 *tile2 = nullptr) {
   using P = Pow2<LOGN, NLINES>;
   using I = TileIdx<LOGN, COLS, NLINES>;
   const int l = I::line();
-  run_stages<LOGN, DIR, 0, COLS, NLINES>(tile + l * P::LP, v, I::bfly(), tw, l);
+  run_stages<LOGN, DIR, 0, COLS, NLINES, DB>(tile + l * P::LP, DB ? tile2 + l * P::LP : nullptr, v, I::bfly(), tw,
+                                             l);
 }
 
 }  // namespace pkde
