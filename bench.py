@@ -45,6 +45,18 @@ def workload(name):
     return x, dict(dims=spec["dims"]), dict(n_bootstraps=64, n_steps=200)
 
 
+def measured_traffic(workload):
+    """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one full-workload
+    engine launch, from the committed ncu summary of that kernel (profiles/); None if
+    there is no capture for this workload."""
+    import re
+    p = os.path.join(REPO, "profiles", "engine_kernel_c2_ncu.md")
+    if workload != "c2" or not os.path.exists(p):
+        return None
+    m = re.search(r"dram_bytes_per_launch_full_c2:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
 def peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -297,8 +309,10 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n * N * 8),
                 "d2h_bytes_per_step": int(G * 12)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
-                     "kernel": "per-bandwidth-step pipeline (step_fft + step_vmr + step_means)",
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": measured_traffic(args.workload) if not args.bandwidth_steps else None,
+                     "algorithmic_bytes": alg_bytes,
+                     "kernel": "engine_kernel (persistent step engine: all bandwidth steps, one launch)",
                      "peak_source": peak_kind, "step_ms_per_estimation": step_ms,
                      "launches_per_estimation": step_launches},
         "phase_ms_per_estimation": {p: v / args.steps for p, v in stats["phase_ms"].items()},

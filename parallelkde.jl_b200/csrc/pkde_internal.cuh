@@ -323,11 +323,20 @@ __device__ __forceinline__ double2 twiddle(const double2 *tw, int m, int dir) {
 
 // One Stockham stage of radix R over `nlines` lines held in shared memory
 // (line pitch `pitch` complex values).  src -> dst.
+// Shared-memory layout of the intermediate buffers: within each aligned block of 8
+// values the index is XOR-swizzled by the block number (i ^ ((i >> 3) & 7)) when n is a
+// multiple of 8.  A first stage (Ns = 1) stores butterfly j's outputs at j*R + q, a
+// stride of R*16 bytes that puts every lane of a quarter-warp in one bank group; the
+// swizzle spreads them over the 8 groups.  The caller-visible input and output buffers
+// keep the plain layout (the first stage reads plain, the last stage writes plain).
+__device__ __forceinline__ int swz(int i, bool on) { return on ? (i ^ ((i >> 3) & 7)) : i; }
+
 // Lines of n < 8192 points and at most 16 lines use the plan's multiply-high divisions
 // for the butterfly indices (their range limits hold there); longer lines divide.
 template <int DIR, int R>
 __device__ __forceinline__ void stockham_stage(const double2 *src, double2 *dst, int n, int pitch,
-                                               int nlines, int Ns, const double2 *tw, FastDiv dnb, FastDiv dns) {
+                                               int nlines, int Ns, const double2 *tw, FastDiv dnb, FastDiv dns,
+                                               bool swz_src, bool swz_dst) {
   const int nb = n / R;
   const int tstep = n / (Ns * R);
   const bool fast = n < 8192 && nlines <= 16;
@@ -340,7 +349,7 @@ __device__ __forceinline__ void stockham_stage(const double2 *src, double2 *dst,
     double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      double2 x = s[j + r * nb];
+      double2 x = s[swz(j + r * nb, swz_src)];
       if (r > 0 && k > 0) x = cmul(x, twiddle(tw, r * k * tstep, DIR));
       v[r] = x;
     }
@@ -352,7 +361,7 @@ __device__ __forceinline__ void stockham_stage(const double2 *src, double2 *dst,
     const int d = jq * Ns * R + k;
     double2 *o = dst + l * pitch;
 #pragma unroll
-    for (int q = 0; q < R; ++q) o[d + q * Ns] = v[q];
+    for (int q = 0; q < R; ++q) o[swz(d + q * Ns, swz_dst)] = v[q];
   }
 }
 
@@ -360,7 +369,7 @@ __device__ __forceinline__ void stockham_stage(const double2 *src, double2 *dst,
 template <int DIR>
 __device__ __forceinline__ void stockham_stage_generic(const double2 *src, double2 *dst, int n,
                                                        int pitch, int nlines, int Ns, int R,
-                                                       const double2 *tw) {
+                                                       const double2 *tw, bool swz_src, bool swz_dst) {
   const int nb = n / R;
   const int tstep = n / (Ns * R);
   for (int t = threadIdx.x; t < nlines * n; t += blockDim.x) {
@@ -374,7 +383,7 @@ __device__ __forceinline__ void stockham_stage_generic(const double2 *src, doubl
     double2 acc = make_double2(0.0, 0.0);
     int m = 0;
     for (int r = 0; r < R; ++r) {
-      double2 x = s[j + r * nb];
+      double2 x = s[swz(j + r * nb, swz_src)];
       double2 w = twiddle(tw, m, DIR);
       acc.x += x.x * w.x - x.y * w.y;
       acc.y += x.x * w.y + x.y * w.x;
@@ -382,7 +391,7 @@ __device__ __forceinline__ void stockham_stage_generic(const double2 *src, doubl
       if (m >= n) m -= n;
     }
     const int d = (j / Ns) * Ns * R + k;
-    dst[l * pitch + d + q * Ns] = acc;
+    dst[l * pitch + swz(d + q * Ns, swz_dst)] = acc;
   }
 }
 
@@ -394,15 +403,17 @@ __device__ double2 *smem_fft(double2 *bufA, double2 *bufB, int pitch, int nlines
   double2 *src = bufA, *dst = bufB;
   int Ns = 1;
   const int n = plan.n;
+  const bool sw = (n & 7) == 0;
   for (int st = 0; st < plan.nstages; ++st) {
     const int R = plan.radix[st];
+    const bool ss = sw && st > 0, sd = sw && st + 1 < plan.nstages;
     switch (R) {
-      case 8: stockham_stage<DIR, 8>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
-      case 4: stockham_stage<DIR, 4>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
-      case 2: stockham_stage<DIR, 2>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
-      case 3: stockham_stage<DIR, 3>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
-      case 5: stockham_stage<DIR, 5>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st]); break;
-      default: stockham_stage_generic<DIR>(src, dst, n, pitch, nlines, Ns, R, tw); break;
+      case 8: stockham_stage<DIR, 8>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st], ss, sd); break;
+      case 4: stockham_stage<DIR, 4>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st], ss, sd); break;
+      case 2: stockham_stage<DIR, 2>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st], ss, sd); break;
+      case 3: stockham_stage<DIR, 3>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st], ss, sd); break;
+      case 5: stockham_stage<DIR, 5>(src, dst, n, pitch, nlines, Ns, tw, plan.div_nb[st], plan.div_ns[st], ss, sd); break;
+      default: stockham_stage_generic<DIR>(src, dst, n, pitch, nlines, Ns, R, tw, ss, sd); break;
     }
     __syncthreads();
     double2 *tmp = src;
