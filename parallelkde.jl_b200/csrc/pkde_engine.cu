@@ -83,6 +83,8 @@ struct EngineEst {
   const double2 *twg[4];       // generic axes: twiddle table (cos, sin)(2 pi m / n), m < n
   FftPlan plan[4];             // generic axes: Stockham radix sequence
   FastDiv dlen[4];             // generic axes: division by the line length
+  int mixr[4];                 // mixed-radix axes (gen 2): R of N = R * 2^logn
+  const double2 *twc[4];       // mixed-radix axes: combine twiddles W_N^(n1 k2), n1 = 1..R-1
 };
 
 // A launch over one or more estimations.  Estimation e runs its local round r in global
@@ -404,6 +406,237 @@ __device__ void means_tile_gen(double2 *smem, const double2 *in, const double *f
   }
 }
 
+// ------------------------------------------------- tile bodies, N = R * 2^LM
+// Axes of N = R * M points (R = 3 or 5, M = 2^LM, 8 <= M <= 256): the line splits into
+// R interleaved sub-lines x[R*n2 + n1] of M points; each goes through the register
+// radix-8 FFT (one butterfly per thread, column mapping over all sub-lines of the tile),
+// then a radix-R combine per output pair: X[k2 + M*q] = sum_n1 W_N^(n1*k2) Y_n1[k2]
+// W_R^(n1*q) (decimation in time at the top level).  The M-point results pass through the
+// tile (same padded layout) to the combine threads.
+__host__ __device__ constexpr int p2floor(int x) { return x < 2 ? 1 : 2 * p2floor(x / 2); }
+
+template <int R, int LM>
+struct Mix {
+  static constexpr int M = 1 << LM;
+  static constexpr int N = R * M;
+  static constexpr int NB8 = M / 8;
+  static constexpr int NLA = p2floor(kEngineThreads / (R * NB8));  // lines per axis-pass tile
+  static constexpr int NLF = NLA > 1 ? NLA / 2 : 1;                 // rows per final-pass tile
+  static_assert(2 * R * NLF * NB8 <= kEngineThreads, "final-pass tile exceeds the block");
+};
+
+// Geometry of one tile: A arrays (1: axis and means passes; 2: z and w of the VMR pass)
+// of NL lines, each line R sub-lines of M points.  Sub-line sub = (a R + n1) NL + l.
+template <int R, int LM, int NL, int A>
+struct MixTile {
+  using X = Mix<R, LM>;
+  static constexpr int SUB = A * R * NL;
+  static constexpr int FT = SUB * X::NB8;                           // threads in the M-point FFTs
+  static constexpr int LPAD = pad8(X::M);
+  static constexpr int LP = LPAD + ((1 - (LPAD % 8)) % 8 + 8) % 8;  // sub-line pitch, 1 mod 8
+  static constexpr int TILE = (SUB + 1) * LP;                       // + a scratch sub-line for idle threads
+  static constexpr int ITEMS = NL * X::M;                           // combine items (per array)
+  static constexpr int PER = (ITEMS + kEngineThreads - 1) / kEngineThreads;
+};
+
+// The calling thread's role in the M-point FFTs: sub-line (array a, phase n1, line l)
+// and butterfly t; threads beyond FT run the scratch sub-line.
+template <class T>
+struct MixRole {
+  bool act;
+  int sub, t, a, n1, l;
+  __device__ __forceinline__ MixRole() {
+    const int tid = threadIdx.x;
+    act = tid < T::FT;
+    sub = act ? tid % T::SUB : T::SUB;
+    t = act ? tid / T::SUB : (tid - T::FT) % T::X::NB8;
+    constexpr int nl = T::ITEMS / T::X::M;
+    constexpr int R = T::X::N / T::X::M;
+    l = sub % nl;
+    n1 = (sub / nl) % R;
+    a = sub / (nl * R);
+  }
+};
+
+// M-point FFTs of the tile's sub-lines (v: the thread's 8 scaled inputs of line positions
+// R * in_pos(t, r) + n1), results into the tile for the combine.  All threads call.
+template <class T>
+__device__ __forceinline__ void mix_fft(double2 *tile, const double2 *sm_tw, const MixRole<T> &ro, double2 (&v)[8]) {
+  constexpr int LM = cilog2(T::X::M);
+  run_stages<LM, 1, 0, true, 0>(tile + ro.sub * T::LP, nullptr, v, ro.t, sm_tw, 0);
+  if (ro.act) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) tile[ro.sub * T::LP + pad8(out_pos<LM>(ro.t, i))] = v[i];
+  }
+  __syncthreads();
+}
+
+// Combine item `it` of the thread for array a: y[q] = X[k2 + M q] of line
+// threadIdx.x % NL.  Returns false when the thread has no such item.
+template <class T>
+__device__ __forceinline__ bool mix_combine(const double2 *tile, const double2 *twc, int it, int a, int &k2,
+                                            double2 (&y)[T::X::N / T::X::M]) {
+  constexpr int R = T::X::N / T::X::M;
+  constexpr int NL = T::ITEMS / T::X::M;
+  const int idx = threadIdx.x + it * kEngineThreads;
+  if (idx >= T::ITEMS) return false;
+  const int l = idx % NL;
+  k2 = idx / NL;
+#pragma unroll
+  for (int n1 = 0; n1 < R; ++n1) {
+    double2 v = tile[((a * R + n1) * NL + l) * T::LP + pad8(k2)];
+    if (n1 > 0) v = cmul(v, __ldg(twc + (n1 - 1) * T::X::M + k2));
+    y[n1] = v;
+  }
+  if constexpr (R == 3) dft3<1>(y);
+  else dft5<1>(y);
+  return true;
+}
+
+template <int R, int LM, bool FROM_SPECTRA>
+__device__ void axis_tiles_mix(double2 *tile, const double2 *sm_tw, const double2 *twc, const double2 *in,
+                               double2 *out, int64_t inner, int64_t first_tile, int ntiles, const double *f) {
+  using X = Mix<R, LM>;
+  using T = MixTile<R, LM, X::NLA, 1>;
+  const MixRole<T> ro;
+  const int lc = threadIdx.x % X::NLA;  // the combine line (NLA divides the block)
+  for (int u = 0; u < ntiles; ++u) {
+    const int64_t L0 = (first_tile + u) * X::NLA;
+    const int64_t Lf = L0 + ro.l, Lc = L0 + lc;
+    const int64_t bf = (Lf / inner) * X::N * inner + (Lf % inner);
+    const int64_t bc = (Lc / inner) * X::N * inner + (Lc % inner);
+    double2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int pos = R * in_pos<LM>(ro.t, r) + ro.n1;
+      const int64_t off = bf + (int64_t)pos * inner;
+      v[r] = ro.act ? cscale(FROM_SPECTRA ? __ldcs(in + off) : __ldcg(in + off), f[pos]) : make_double2(0.0, 0.0);
+    }
+    mix_fft<T>(tile, sm_tw, ro, v);
+#pragma unroll
+    for (int it = 0; it < T::PER; ++it) {
+      int k2;
+      double2 y[R];
+      if (mix_combine<T>(tile, twc, it, 0, k2, y)) {
+#pragma unroll
+        for (int q = 0; q < R; ++q) __stcg(out + bc + (int64_t)(k2 + X::M * q) * inner, y[q]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Final pass: NLF rows; the tile holds the z and the w sub-lines of those rows, so each
+// combine item has both transforms of its points for the VMR and the Welford update.
+template <int R, int LM>
+__device__ void vmr_tile_mix(double2 *tile, double2 *state, const double2 *sm_tw, const double2 *twc,
+                             const double2 *in, int npairs, int b0, int nboot, const double *fz, const double *fw,
+                             double cz, double cw, double inv_n, int64_t G, double *wst, int first, int64_t tile_idx) {
+  using X = Mix<R, LM>;
+  using T = MixTile<R, LM, X::NLF, 2>;
+  const MixRole<T> ro;
+  const int npts = X::NLF * X::N;
+  const int64_t rbase = tile_idx * npts;
+  const int lrow = (threadIdx.x % X::NLF) * X::N;
+  for (int e = threadIdx.x; e < npts; e += blockDim.x)
+    state[e] = first ? make_double2(0.0, 0.0) : make_double2(__ldcg(wst + rbase + e), __ldcg(wst + G + rbase + e));
+  for (int p = 0; p < npairs; ++p) {
+    const double2 *src = in + (int64_t)(2 * p + ro.a) * G + rbase + ro.l * X::N;
+    const double *f = ro.a ? fw : fz;
+    const double c = ro.a ? cw : cz;
+    double2 v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int pos = R * in_pos<LM>(ro.t, r) + ro.n1;
+      v[r] = ro.act ? cscale(__ldcg(src + pos), c * f[pos]) : make_double2(0.0, 0.0);
+    }
+    mix_fft<T>(tile, sm_tw, ro, v);
+    const int b = b0 + 2 * p;
+    const double inv_a = 1.0 / (double)(b + 1), inv_b = 1.0 / (double)(b + 2);
+    const bool has_b = b + 1 < nboot;
+#pragma unroll
+    for (int it = 0; it < T::PER; ++it) {
+      int k2;
+      double2 z[R], w[R];
+      if (mix_combine<T>(tile, twc, it, 0, k2, z)) {
+        mix_combine<T>(tile, twc, it, 1, k2, w);
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int e = lrow + k2 + X::M * q;
+          double2 st = state[e];
+          welford(vmr_of(z[q].x, w[q].x, inv_n), inv_a, st.x, st.y);
+          if (has_b) welford(vmr_of(z[q].y, w[q].y, inv_n), inv_b, st.x, st.y);
+          state[e] = st;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < npts; e += blockDim.x) {
+    const double2 st = state[e];
+    __stcg(wst + rbase + e, st.x);
+    __stcg(wst + G + rbase + e, st.y);
+  }
+}
+
+// Means pass over the same NLF rows (one array; the second array's threads idle).
+template <int R, int LM>
+__device__ void means_tile_mix(double2 *tile, const double2 *sm_tw, const double2 *twc, const double2 *in,
+                               const double *fz, double cz, const double *wst, int64_t G, int nboot, double vscale,
+                               double dlogt, double eps, int64_t steps_low, int64_t steps_over, const StepState &cs,
+                               int step, int64_t tile_idx) {
+  using X = Mix<R, LM>;
+  using T = MixTile<R, LM, X::NLF, 1>;
+  const MixRole<T> ro;
+  const int64_t rbase = tile_idx * (X::NLF * X::N);
+  const int lrow = (threadIdx.x % X::NLF) * X::N;
+  const double2 *src = in + rbase + ro.l * X::N;
+  double2 v[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int pos = R * in_pos<LM>(ro.t, r) + ro.n1;
+    v[r] = ro.act ? cscale(__ldcg(src + pos), cz * fz[pos]) : make_double2(0.0, 0.0);
+  }
+  mix_fft<T>(tile, sm_tw, ro, v);
+#pragma unroll
+  for (int it = 0; it < T::PER; ++it) {
+    int k2;
+    double2 y[R];
+    if (mix_combine<T>(tile, twc, it, 0, k2, y)) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int64_t gi = rbase + lrow + k2 + X::M * q;
+        const double mu = sqrt(y[q].x * y[q].x + y[q].y * y[q].y);
+        const double m2 = __ldcg(wst + G + gi);
+        step_update<true>(cs, gi, mu, vscale * m2 / (double)(nboot - 1), dlogt, eps, steps_low, steps_over, step);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+#define PKDE_MIX_SWITCH(R, LM, CALL)                                                     \
+  if (R == 3) {                                                                          \
+    switch (LM) {                                                                        \
+      case 3: CALL(3, 3); break;                                                         \
+      case 4: CALL(3, 4); break;                                                         \
+      case 5: CALL(3, 5); break;                                                         \
+      case 6: CALL(3, 6); break;                                                         \
+      case 7: CALL(3, 7); break;                                                         \
+      case 8: CALL(3, 8); break;                                                         \
+      default: break;                                                                    \
+    }                                                                                    \
+  } else {                                                                               \
+    switch (LM) {                                                                        \
+      case 3: CALL(5, 3); break;                                                         \
+      case 4: CALL(5, 4); break;                                                         \
+      case 5: CALL(5, 5); break;                                                         \
+      case 6: CALL(5, 6); break;                                                         \
+      case 7: CALL(5, 7); break;                                                         \
+      default: break;                                                                    \
+    }                                                                                    \
+  }
+
 // ------------------------------------------------------------------ the engine
 #define PKDE_ENGINE_SWITCH(LN, CALL) \
   switch (LN) {                      \
@@ -547,17 +780,28 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
     else                                                                                  \
       axis_tiles<L, false>(tile_mem, state, sm_tw, in, out, inner, first_tile, tpi, f);   \
   }
-      if (GEN && E.gen[a]) {
+#define PKDE_AXIS_MIX(RR, LL)                                                                   \
+  {                                                                                             \
+    stage_tw<LL>(sm_tw, R.tw[LL], cached_tw, LL);                                               \
+    if (p == 0)                                                                                 \
+      axis_tiles_mix<RR, LL, true>(tile_mem, sm_tw, E.twc[a], in, out, inner, first_tile, tpi, f); \
+    else                                                                                        \
+      axis_tiles_mix<RR, LL, false>(tile_mem, sm_tw, E.twc[a], in, out, inner, first_tile, tpi, f); \
+  }
+      if (GEN && E.gen[a] == 1) {
         if (p == 0)
           axis_tiles_gen<true>(tile_mem, in, out, (int)E.dims[a], inner, first_tile, tpi, f, E.tl[a], E.plan[a],
                                E.twg[a]);
         else
           axis_tiles_gen<false>(tile_mem, in, out, (int)E.dims[a], inner, first_tile, tpi, f, E.tl[a], E.plan[a],
                                 E.twg[a]);
+      } else if (GEN && E.gen[a] == 2) {
+        PKDE_MIX_SWITCH(E.mixr[a], ln, PKDE_AXIS_MIX)
       } else {
         PKDE_ENGINE_SWITCH(ln, PKDE_AXIS)
       }
 #undef PKDE_AXIS
+#undef PKDE_AXIS_MIX
     } else {
       const int ln = E.logn[0];
       if (!means) {
@@ -569,7 +813,16 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
                 fws + E.aoff[0], E.invG, E.invG * E.cw[s], E.inv_n, E.G, E.wstate + (s & 1) * 2 * E.G,      \
                 j == 0, tile);                                                                              \
   }
-        if (GEN && E.gen[0]) {
+#define PKDE_VMR_MIX(RR, LL)                                                                              \
+  {                                                                                                       \
+    stage_tw<LL>(sm_tw, R.tw[LL], cached_tw, LL);                                                         \
+    vmr_tile_mix<RR, LL>(tile_mem, state, sm_tw, E.twc[0], slot_base, np, 2 * j * E.g, E.nboot,            \
+                         fzs + E.aoff[0], fws + E.aoff[0], E.invG, E.invG * E.cw[s], E.inv_n, E.G,         \
+                         E.wstate + (s & 1) * 2 * E.G, j == 0, tile);                                      \
+  }
+        if (GEN && E.gen[0] == 2) {
+          PKDE_MIX_SWITCH(E.mixr[0], ln, PKDE_VMR_MIX)
+        } else if (GEN && E.gen[0]) {
           vmr_tile_gen(tile_mem, state, slot_base, np, 2 * j * E.g, E.nboot, fzs + E.aoff[0], fws + E.aoff[0], E.invG,
                        E.invG * E.cw[s], E.inv_n, E.G, E.wstate + (s & 1) * 2 * E.G, j == 0, tile, (int)E.dims[0],
                        E.tl[0], E.plan[0], E.twg[0], E.dlen[0]);
@@ -577,6 +830,7 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
           PKDE_ENGINE_SWITCH(ln, PKDE_VMR)
         }
 #undef PKDE_VMR
+#undef PKDE_VMR_MIX
       } else {
 #define PKDE_MEANS(L)                                                                                        \
   {                                                                                                          \
@@ -584,7 +838,16 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
     means_tile<L>(tile_mem, sm_tw, slot_base, fzs + E.aoff[0], E.invG, E.wstate + (s & 1) * 2 * E.G, E.G,     \
                   E.nboot, E.vscale[s], E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs, (int)s, tile);   \
   }
-        if (GEN && E.gen[0]) {
+#define PKDE_MEANS_MIX(RR, LL)                                                                          \
+  {                                                                                                     \
+    stage_tw<LL>(sm_tw, R.tw[LL], cached_tw, LL);                                                       \
+    means_tile_mix<RR, LL>(tile_mem, sm_tw, E.twc[0], slot_base, fzs + E.aoff[0], E.invG,                \
+                           E.wstate + (s & 1) * 2 * E.G, E.G, E.nboot, E.vscale[s], E.dlogt[s], E.eps,   \
+                           E.steps_low, E.steps_over, E.cs, (int)s, tile);                               \
+  }
+        if (GEN && E.gen[0] == 2) {
+          PKDE_MIX_SWITCH(E.mixr[0], ln, PKDE_MEANS_MIX)
+        } else if (GEN && E.gen[0]) {
           means_tile_gen(tile_mem, slot_base, fzs + E.aoff[0], E.invG, E.wstate + (s & 1) * 2 * E.G, E.G, E.nboot,
                          E.vscale[s], E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs, (int)s, tile,
                          (int)E.dims[0], E.tl[0], E.plan[0], E.twg[0], E.dlen[0]);
@@ -592,6 +855,7 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
           PKDE_ENGINE_SWITCH(ln, PKDE_MEANS)
         }
 #undef PKDE_MEANS
+#undef PKDE_MEANS_MIX
       }
     }
     // ---- signal completion
@@ -642,6 +906,44 @@ int engine_env_int(const char *name, int dflt, int lo, int hi) {
   return x < lo ? lo : (x > hi ? hi : x);
 }
 
+#define PKDE_MIX_HOST(RR, LL) return fn(Mix<RR, LL>{});
+template <class F>
+static size_t mix_dispatch(int R, int lm, F fn) {
+  PKDE_MIX_SWITCH(R, lm, PKDE_MIX_HOST)
+  return 0;
+}
+#undef PKDE_MIX_HOST
+// lines per tile: axis passes (axis >= 2) and the final pass (axis 1)
+static int mix_lines(int R, int lm, bool final_pass) {
+  return (int)mix_dispatch(R, lm, [&](auto x) { return (size_t)(final_pass ? decltype(x)::NLF : decltype(x)::NLA); });
+}
+static size_t mix_tile_elems(int R, int lm) {
+  return mix_dispatch(R, lm, [](auto x) {
+    using X = decltype(x);
+    constexpr int R_ = X::N / X::M, LM_ = cilog2(X::M);
+    return std::max<size_t>(MixTile<R_, LM_, X::NLA, 1>::TILE, MixTile<R_, LM_, X::NLF, 2>::TILE);
+  });
+}
+
+// Combine twiddles of N = R * M: (cos, sin)(2 pi n1 k2 / N), n1 = 1..R-1, k2 < M.
+static const double2 *combine_twiddles_device(pkde_ctx *ctx, int R, int M) {
+  const int N = R * M;
+  const int key = -(1000000 + 10 * N + R);
+  auto it = ctx->twiddles.find(key);
+  if (it != ctx->twiddles.end()) return it->second.as<double2>();
+  std::vector<double2> tw;
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int n1 = 1; n1 < R; ++n1)
+    for (int k2 = 0; k2 < M; ++k2) {
+      const long double a = two_pi * (long double)((n1 * k2) % N) / (long double)N;
+      tw.push_back(make_double2((double)cosl(a), (double)sinl(a)));
+    }
+  DevBuf &b = ctx->twiddles[key];
+  b.ensure(sizeof(double2) * tw.size());
+  PKDE_CUDA_TRY(cudaMemcpy(b.ptr, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice));
+  return b.as<double2>();
+}
+
 // Tile shape of grid axis j: the register radix-8 FFT where the axis is a power of two
 // in 16..8*kEngineThreads whose tiles line up with the layout; otherwise the
 // shared-memory mixed-radix FFT for lengths up to 8*kEngineThreads, TL lines per tile
@@ -661,6 +963,15 @@ static AxisShape axis_shape(const pkde_grid *g, int j) {
   if (ln >= 4 && (int64_t(1) << ln) <= 8 * kEngineThreads) {
     const int nl = tile_lines_of(ln);
     if (lines % nl == 0 && (j == 0 || inner % nl == 0)) return AxisShape{true, 0, nl};
+  }
+  // N = R * 2^LM, R = 3 or 5, M = 2^LM in 8..256 (R = 3) or 8..128 (R = 5): mixed-radix
+  // register tiles when their lines per tile divide the number of lines
+  for (int R : {3, 5}) {
+    if (n % R) continue;
+    const int lm = ilog2_pow2(n / R);
+    if (lm < 3 || lm > (R == 3 ? 8 : 7)) continue;
+    const int nl = mix_lines(R, lm, j == 0);
+    if (lines % nl == 0) return AxisShape{true, 2, nl};
   }
   if (n < 2 || n > 8 * kEngineThreads) return AxisShape{false, 0, 0};
   int tl = 1;
@@ -691,7 +1002,13 @@ EngineEst describe(const EngineArgs &A) {
     E.dims[j] = g->dims[j];
     E.gen[j] = sh.gen;
     E.tl[j] = sh.tl;
-    E.logn[j] = sh.gen ? -1 : ilog2_pow2(g->dims[j]);
+    E.mixr[j] = 0;
+    if (sh.gen == 2) {
+      E.mixr[j] = g->dims[j] % 3 == 0 && ilog2_pow2(g->dims[j] / 3) >= 3 ? 3 : 5;
+      E.logn[j] = ilog2_pow2(g->dims[j] / E.mixr[j]);
+    } else {
+      E.logn[j] = sh.gen ? -1 : ilog2_pow2(g->dims[j]);
+    }
     E.aoff[j] = A.aoff[j];
   }
   E.npairs = A.npairs;
@@ -747,7 +1064,12 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
     EngineEst &E = est[e];
     E = describe(args[e]);
     for (int j = 0; j < E.ndim; ++j) {
-      if (E.gen[j]) {
+      if (E.gen[j] == 2) {
+        R.tw[E.logn[j]] = stage_twiddles_device(ctx, E.logn[j]);
+        E.twc[j] = combine_twiddles_device(ctx, E.mixr[j], 1 << E.logn[j]);
+        max_tile = std::max(max_tile, mix_tile_elems(E.mixr[j], E.logn[j]));
+        max_tw = std::max(max_tw, tw_elems(E.logn[j]));
+      } else if (E.gen[j]) {
         E.twg[j] = twiddles_device(ctx, (int)E.dims[j]);
         E.plan[j] = make_plan((int)E.dims[j]);
         E.dlen[j] = make_fastdiv((uint32_t)E.dims[j]);

@@ -171,7 +171,10 @@ def _compare(pk, oracle, data, og_grid, B, n_steps=None, idx_seed=5, **kw):
                                                    (3, (16, 20, 12), 20000, 6, 30), (4, (8, 6, 10, 7), 20000, 4, 20),
                                                    (2, (64, 32), 20000, 8, 40), (2, (256, 128), 50000, 5, 30),
                                                    (3, (16, 32, 16), 20000, 6, 30), (2, (2048, 16), 20000, 4, 20),
-                                                   (4, (16, 16, 16, 16), 30000, 4, 12)])
+                                                   (4, (16, 16, 16, 16), 30000, 4, 12),
+                                                   # mixed-radix engine tiles (N = 3 or 5 times a power of two)
+                                                   (2, (96, 80), 30000, 6, 30), (2, (24, 320), 20000, 4, 20),
+                                                   (3, (48, 40, 24), 30000, 4, 15), (2, (384, 192), 40000, 4, 12)])
 def test_estimate_matches_oracle(pk, oracle, n_dims, dims, n, B, steps):
     rng = np.random.default_rng(10 + n_dims)
     data = rng.standard_normal((n_dims, n))
