@@ -1024,7 +1024,9 @@ EngineEst describe(const EngineArgs &A) {
   E.J = (E.npairs + E.g - 1) / E.g;
   // pipeline delay between passes of one batch; ring slots cover the delay
   E.D = A.tune_delay > 0 ? A.tune_delay : engine_env_int("PKDE_ENGINE_DELAY", 2, 1, 8);
-  E.Q = (E.P - 1) * E.D + 2;
+  // ring slots: the pipeline depth plus a margin (extra slots let pass 0 of a batch start
+  // before the final pass of the batch Q earlier has released its slot)
+  E.Q = (E.P - 1) * E.D + 2 + (A.tune_qextra > 0 ? A.tune_qextra : engine_env_int("PKDE_ENGINE_QEXTRA", 0, 0, 8));
   E.NB = (int64_t)E.S * (E.J + 1);
   E.Tf = (int)((E.G / E.dims[0]) / E.tl[0]);
   for (int a = 0; a < 4; ++a) E.tpi[a] = 1;

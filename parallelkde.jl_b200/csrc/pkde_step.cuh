@@ -139,7 +139,7 @@ struct EngineArgs {
   StepState cs;
   // schedule parameters (0: default): ring-slot MB, tiles per axis-pass item, pipeline
   // delay between the passes of a batch
-  int tune_slot_mb = 0, tune_tpi = 0, tune_delay = 0;
+  int tune_slot_mb = 0, tune_tpi = 0, tune_delay = 0, tune_qextra = 0;
 };
 bool engine_ok(const pkde_grid *g);
 // Per-shape schedule parameters: from the context's cache, else (autotuning on) timed

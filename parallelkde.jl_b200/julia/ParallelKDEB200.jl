@@ -21,7 +21,7 @@ module ParallelKDEB200
 
 using CUDA
 using ParallelKDE
-using ParallelKDE.DensityEstimators: AbstractGradeProEstimator
+using ParallelKDE.DensityEstimators: AbstractGradeProEstimator, AbstractRoTEstimator
 import ParallelKDE.DensityEstimators: estimate!
 
 const libpkde = joinpath(@__DIR__, "..", "lib", "libpkde_b200.so")
@@ -117,6 +117,66 @@ function estimate!(::Type{AbstractGradeProEstimator}, kde::ParallelKDE.KDEs.CuKD
     check(rc, ctx)
     copyto!(kde.density, dens)
     return nothing
+end
+
+"""
+    estimate!(::Type{AbstractRoTEstimator}, kde::CuKDE; grid, rule_of_thumb=:scott)
+
+The `device=:cuda` path of `estimate_density!(est, :rot)` (RoTEstimator.jl:117-201) on
+libpkde_b200: identity binning, FFT, one propagation by the rule-of-thumb bandwidth minus
+h/2, inverse FFT, `abs`.
+"""
+function estimate!(::Type{AbstractRoTEstimator}, kde::ParallelKDE.KDEs.CuKDE;
+                   method::Union{Nothing,Symbol}=nothing, grid, rule_of_thumb::Symbol=:scott,
+                   device::Integer=CUDA.device().handle, kwargs...)
+    method === nothing || method == :cuda ||
+        throw(ArgumentError("Invalid implementation $method for device IsCUDA()"))
+    rule = rule_of_thumb === :scott ? Int32(0) : rule_of_thumb === :silverman ? Int32(1) :
+           throw(ArgumentError("Rule of thumb $rule_of_thumb not implemented."))
+    data = CuArray{Float64}(kde.data)
+    dens = CuArray{Float64}(undef, size(kde.density))
+    ctx = context(device)
+    rc = ccall((:pkde_rot_estimate, libpkde), Cint,
+               (Ptr{Cvoid}, Ref{PkdeGrid}, Int32, CuPtr{Float64}, Int64, CuPtr{Float64}, UInt32, Ptr{Cvoid}),
+               ctx, grid_struct(grid), rule, data, size(data, 2), dens,
+               PKDE_DEVICE_INPUT | PKDE_DEVICE_OUTPUT, CUDA.stream().handle)
+    check(rc, ctx)
+    copyto!(kde.density, dens)
+    return nothing
+end
+
+"""
+    find_grid_device(data::CuMatrix; dims=nothing, padding=nothing) -> (lo, hi, dims, h)
+
+find_grid (Grids.jl:252-300) with the extrema reduced on the GPU (pkde_find_grid); the
+caller builds its CuGrid from the returned ranges.
+"""
+function find_grid_device(data::CuMatrix{Float64}; dims=nothing, padding=nothing, device::Integer=CUDA.device().handle)
+    N = size(data, 1)
+    g = Ref(PkdeGrid(Int32(0), Int32(0), (0, 0, 0, 0), (0.0, 0.0, 0.0, 0.0), (0.0, 0.0, 0.0, 0.0), (0.0, 0.0, 0.0, 0.0)))
+    d = dims === nothing ? C_NULL : Int64[dims...]
+    pd = padding === nothing ? C_NULL : Float64[padding...]
+    ctx = context(device)
+    rc = ccall((:pkde_find_grid, libpkde), Cint,
+               (Ptr{Cvoid}, Int32, CuPtr{Float64}, Int64, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}, Ref{PkdeGrid},
+                UInt32, Ptr{Cvoid}),
+               ctx, Int32(N), data, size(data, 2), d, C_NULL, pd, g, PKDE_DEVICE_INPUT, CUDA.stream().handle)
+    check(rc, ctx)
+    G = g[]
+    return (G.lo[1:N], G.hi[1:N], G.dims[1:N], G.h[1:N])
+end
+
+"""
+    normalize_density!(density::CuArray{Float64}, dx)
+
+get_density(...; normalize=true) (ParallelKDE.jl:189-202) in place on the device, FP64 sum.
+"""
+function normalize_density!(density::CuArray{Float64}, dx::Real; device::Integer=CUDA.device().handle)
+    ctx = context(device)
+    rc = ccall((:pkde_normalize_density, libpkde), Cint, (Ptr{Cvoid}, CuPtr{Float64}, Int64, Float64, UInt32, Ptr{Cvoid}),
+               ctx, density, length(density), Float64(dx), PKDE_DEVICE_INPUT, CUDA.stream().handle)
+    check(rc, ctx)
+    return density
 end
 
 end # module
