@@ -921,7 +921,8 @@ static size_t mix_tile_elems(int R, int lm) {
   return mix_dispatch(R, lm, [](auto x) {
     using X = decltype(x);
     constexpr int R_ = X::N / X::M, LM_ = cilog2(X::M);
-    return std::max<size_t>(MixTile<R_, LM_, X::NLA, 1>::TILE, MixTile<R_, LM_, X::NLF, 2>::TILE);
+    return std::max<size_t>({MixTile<R_, LM_, X::NLA, 1>::TILE, MixTile<R_, LM_, X::NLF, 2>::TILE,
+                             MixTile<R_, LM_, X::NLF, 1>::TILE});
   });
 }
 

@@ -324,7 +324,6 @@ Ladder make_ladder(const pkde_gradepro_params *p, const double *bw_final, int64_
   }
   const long double n3 = (long double)n_samples * (long double)n_samples * (long double)n_samples;
   const double n3d = (double)n3;  // n^3 rounded once (exact in long double up to 2^64)
-  const int64_t B = p->n_bootstraps;
   L.dlogt.resize(L.S);
   L.vscale.resize(L.S);
   L.cw.resize(L.S);
