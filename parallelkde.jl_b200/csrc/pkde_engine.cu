@@ -988,6 +988,12 @@ bool engine_ok(const pkde_grid *g) {
   return true;
 }
 
+bool engine_register_only(const pkde_grid *g) {
+  for (int j = 0; j < g->ndim; ++j)
+    if (axis_shape(g, j).gen) return false;
+  return true;
+}
+
 namespace {
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }

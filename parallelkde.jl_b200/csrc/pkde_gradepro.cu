@@ -759,7 +759,6 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
            PKDE_PHASE_FORWARD_FFT);
   // ---- bandwidth steps
   std::vector<EngineArgs> eng;
-  std::vector<int> eng_who;
   for (int e = 0; e < count; ++e) {
     Plan &P = plans[e];
     const Ladder &L = P.L;
@@ -812,9 +811,16 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
     autotune_engine(ctx, A, st);  // trial runs (if any) overwrite the state: initialise after
     init_state();
     eng.push_back(A);
-    eng_who.push_back(e);
   }
-  if (!eng.empty()) run_engine_batch(ctx, eng.data(), (int)eng.size(), st);
+  // two persistent launches: estimations whose axes all take the register power-of-two
+  // tiles run in the lean kernel instantiation, the others in the one with the
+  // mixed-radix and shared-memory tiles (more registers spilled)
+  {
+    std::vector<EngineArgs> lean, wide;
+    for (const EngineArgs &A : eng) (engine_register_only(A.grid) ? lean : wide).push_back(A);
+    if (!lean.empty()) run_engine_batch(ctx, lean.data(), (int)lean.size(), st);
+    if (!wide.empty()) run_engine_batch(ctx, wide.data(), (int)wide.size(), st);
+  }
   // ---- replace_nans! and outputs
   for (int e = 0; e < count; ++e) {
     Plan &P = plans[e];

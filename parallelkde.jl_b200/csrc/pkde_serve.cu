@@ -156,9 +156,16 @@ Server *start_server(pkde_ctx *ctx) {
   S->lane_bytes = ctx->serve_lane_bytes > 0 ? (size_t)ctx->serve_lane_bytes : (size_t)(0.8 * (double)freeb / lanes);
   for (int i = 0; i < lanes; ++i) {
     pkde_ctx *c = nullptr;
-    if (pkde_create(&c, ctx->device) != PKDE_OK) throw Error{PKDE_ECUDA, "serving: cannot create a lane context"};
-    cudaStream_t s;
-    PKDE_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaStream_t s = nullptr;
+    if (pkde_create(&c, ctx->device) != PKDE_OK || cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      if (c) pkde_destroy(c);
+      for (size_t k = 0; k < S->lane_ctx.size(); ++k) {
+        cudaStreamDestroy(S->lane_stream[k]);
+        pkde_destroy(S->lane_ctx[k]);
+      }
+      delete S;
+      throw Error{PKDE_ECUDA, "serving: cannot create a lane context or stream"};
+    }
     S->lane_ctx.push_back(c);
     S->lane_stream.push_back(s);
   }

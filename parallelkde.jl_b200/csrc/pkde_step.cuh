@@ -142,6 +142,8 @@ struct EngineArgs {
   int tune_slot_mb = 0, tune_tpi = 0, tune_delay = 0, tune_qextra = 0;
 };
 bool engine_ok(const pkde_grid *g);
+// Every axis on the register power-of-two tiles (the engine's lean instantiation).
+bool engine_register_only(const pkde_grid *g);
 // Per-shape schedule parameters: from the context's cache, else (autotuning on) timed
 // trial runs of the estimation's first bandwidth steps.  Overwrites the estimation's
 // convergence state (the caller initialises it afterwards).
