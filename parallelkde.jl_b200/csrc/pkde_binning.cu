@@ -173,6 +173,197 @@ __global__ void weight_kernel(const uint32_t *__restrict__ cell, int64_t n, int6
   }
 }
 
+// ---------------------------------------------------------------------------
+// Estimator scatter in cell order.  The samples are sorted by lower cell once (a counting
+// sort from the identity counts); each bootstrap's draws become per-sample
+// multiplicities m[b][i] (i = position in cell order); the scatter then walks (b, i) in
+// order and adds m * term.  Neighbouring threads hit neighbouring cells, and within a
+// warp the contributions of equal cells are summed (segmented scan) before one atomic.
+// All sums are exact 64-bit integers, so the result equals the per-draw scatter's.
+
+constexpr int kScanChunk = 2048;  // cells per block in the scans
+
+// per-chunk sums of the identity counts (the samples per cell)
+__global__ void cell_chunk_sum_kernel(const uint32_t *__restrict__ cnt, int64_t G, uint32_t *__restrict__ csum) {
+  __shared__ uint32_t sh[kThreads / 32];
+  const int64_t c0 = (int64_t)blockIdx.x * kScanChunk;
+  uint32_t v = 0;
+  for (int k = threadIdx.x; k < kScanChunk; k += blockDim.x)
+    if (c0 + k < G) v += cnt[c0 + k];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < kThreads / 32; ++w) t += sh[w];
+    csum[blockIdx.x] = t;
+  }
+}
+
+// exclusive scan of the chunk sums (one block, in order)
+__global__ void chunk_scan_kernel(uint32_t *csum, int64_t nchunks) {
+  if (threadIdx.x != 0) return;
+  uint32_t run = 0;
+  for (int64_t k = 0; k < nchunks; ++k) {
+    const uint32_t v = csum[k];
+    csum[k] = run;
+    run += v;
+  }
+}
+
+// cstart[c] = first position of cell c in cell order (exclusive scan of the counts);
+// also clears the per-cell fill counters
+__global__ void cell_start_kernel(const uint32_t *__restrict__ cnt, int64_t G, const uint32_t *__restrict__ csum,
+                                  uint32_t *__restrict__ cstart, uint32_t *__restrict__ cfill) {
+  __shared__ uint32_t part[kThreads];
+  const int64_t c0 = (int64_t)blockIdx.x * kScanChunk;
+  constexpr int PER = kScanChunk / kThreads;
+  uint32_t v[PER];
+  uint32_t t = 0;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int64_t c = c0 + threadIdx.x * PER + q;
+    v[q] = c < G ? cnt[c] : 0u;
+    t += v[q];
+  }
+  part[threadIdx.x] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {  // exclusive scan of the per-thread sums (256 values)
+    uint32_t run = csum[blockIdx.x];
+    for (int k = 0; k < kThreads; ++k) {
+      const uint32_t x = part[k];
+      part[k] = run;
+      run += x;
+    }
+  }
+  __syncthreads();
+  uint32_t run = part[threadIdx.x];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int64_t c = c0 + threadIdx.x * PER + q;
+    if (c < G) {
+      cstart[c] = run;
+      cfill[c] = 0u;
+    }
+    run += v[q];
+  }
+}
+
+// pos[s] = position of sample s in cell order; cell_sorted[pos] = its lower cell
+__global__ void cell_sort_kernel(const uint32_t *__restrict__ cell, int64_t n, const uint32_t *__restrict__ cstart,
+                                 uint32_t *__restrict__ cfill, uint32_t *__restrict__ pos,
+                                 uint32_t *__restrict__ cell_sorted) {
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = cell[s];
+    const uint32_t p = cstart[c] + atomicAdd(&cfill[c], 1u);
+    pos[s] = p;
+    cell_sorted[p] = c;
+  }
+}
+
+// mult[b * n + pos[s]] = how often resample b draws sample s
+__global__ void mult_kernel(int64_t n, int64_t nboot, const int32_t *__restrict__ idx, uint64_t seed,
+                            const uint32_t *__restrict__ pos, uint32_t *__restrict__ mult, int *err) {
+  const int64_t total = nboot * n;
+  for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d < total; d += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = d / n;
+    const int64_t j = d - b * n;
+    const int64_t s = draw_sample(b, j, n, nboot, idx, seed, err);
+    atomicAdd(&mult[b * n + pos[s]], 1u);
+  }
+}
+
+// The quantised corner terms of DirectSpace.jl:227-237, stored at the sample's position
+// in cell order (quantize_kernel's arithmetic).
+__global__ void quantize_sorted_kernel(GridDev g, const double *__restrict__ rh, int64_t n, double denom, int e_m,
+                                       int e_v, const uint32_t *__restrict__ pos, unsigned long long *__restrict__ qm,
+                                       unsigned long long *__restrict__ qv) {
+  int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const int N = g.ndim;
+  const int64_t ps = pos[s];
+  double r_h[4], r_l[4];
+  for (int j = 0; j < N; ++j) {
+    r_h[j] = rh[j * n + s];
+    r_l[j] = __dsub_rn(g.h[j], r_h[j]);
+  }
+  const int nc = 1 << N;
+  for (int c = 0; c < nc; ++c) {
+    double pl = 1.0, ph = 1.0;
+    bool fl = false, fh = false;
+    for (int j = 0; j < N; ++j) {
+      if ((c >> (N - 1 - j)) & 1) {
+        pl = fl ? __dmul_rn(pl, r_l[j]) : r_l[j];
+        fl = true;
+      } else {
+        ph = fh ? __dmul_rn(ph, r_h[j]) : r_h[j];
+        fh = true;
+      }
+    }
+    double term = __ddiv_rn(__dmul_rn(pl, ph), denom);
+    double sq = __dmul_rn(term, term);
+    qm[c * n + ps] = __double2ull_rn(ldexp(term, e_m));
+    qv[c * n + ps] = __double2ull_rn(ldexp(sq, e_v));
+  }
+}
+
+// Scatter in cell order into the paired spectra slots.  Work item d = (b, i), b-major,
+// b = nboot the identity (multiplicity 1).  Warp lanes hold consecutive items: keys
+// (b, cell) are non-decreasing along the warp, so equal keys are contiguous and an
+// inclusive segmented scan sums each run; the run's last lane adds it with one atomic.
+template <int N>
+__global__ void weight_sorted_kernel(const uint32_t *__restrict__ cell_sorted, int64_t n, int64_t nboot, int64_t G,
+                                     const int64_t *__restrict__ corner_off, const uint32_t *__restrict__ mult,
+                                     const unsigned long long *__restrict__ qm,
+                                     const unsigned long long *__restrict__ qv, unsigned long long *__restrict__ out,
+                                     int64_t npairs) {
+  constexpr int nc = 1 << N;
+  const int lane = threadIdx.x & 31;
+  const int64_t total = (nboot + 1) * n;
+  // every lane of a warp runs the same number of iterations (the loop bound is rounded
+  // up to whole warps), so the shuffles always see all 32 lanes
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d - lane < total; d += stride) {
+    const bool act = d < total;
+    const int64_t b = act ? d / n : 0;
+    const int64_t i = act ? d - b * n : 0;
+    const uint32_t m = act ? (b == nboot ? 1u : mult[b * n + i]) : 0u;
+    const uint32_t c0 = act ? cell_sorted[i] : 0u;
+    const unsigned long long key = act ? (((unsigned long long)b << 32) | c0) : ~0ull - (unsigned long long)lane;
+    bool same[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const unsigned long long up = __shfl_up_sync(0xffffffffu, key, 1 << k);
+      same[k] = lane >= (1 << k) && up == key;
+    }
+    const bool last = __shfl_down_sync(0xffffffffu, key, 1) != key || lane == 31;
+    const int64_t p = b >> 1, half = b & 1;
+#pragma unroll
+    for (int c = 0; c < nc; ++c) {
+      const int64_t cc = (int64_t)c0 + (act ? corner_off[c] : 0);
+      unsigned long long vm = m ? (unsigned long long)m * qm[c * n + i] : 0ull;
+      unsigned long long vv = (m && b < nboot) ? (unsigned long long)m * qv[c * n + i] : 0ull;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const unsigned long long um = __shfl_up_sync(0xffffffffu, vm, 1 << k);
+        const unsigned long long uv = __shfl_up_sync(0xffffffffu, vv, 1 << k);
+        if (same[k]) {
+          vm += um;
+          vv += uv;
+        }
+      }
+      if (act && last) {
+        if (b == nboot) {
+          if (vm) atomicAdd(&out[(2 * npairs * G + cc) * 2], vm);
+        } else {
+          if (vm) atomicAdd(&out[((2 * p) * G + cc) * 2 + half], vm);
+          if (vv) atomicAdd(&out[((2 * p + 1) * G + cc) * 2 + half], vv);
+        }
+      }
+    }
+  }
+}
+
 // In-place conversion of the fixed-point sums to FP64 (same 8-byte slots).
 __global__ void dequant_kernel(unsigned long long *v, int64_t m, double scale) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
@@ -337,22 +528,36 @@ size_t dirac_job_scratch(const pkde_grid *g, int64_t n, int64_t nboot) {
   const int N = g->ndim;
   const int64_t nc = int64_t(1) << N;
   const int64_t G = grid_size(g);
+  const int64_t nchunk = (G + kScanChunk - 1) / kScanChunk;
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   return al(sizeof(uint32_t) * n) + al(sizeof(double) * N * n + sizeof(unsigned long long) * 2 * nc * n) +
-         al(sizeof(uint32_t) * (nboot + 1) * G);
+         al(sizeof(uint32_t) * (nboot + 1) * G) + 2 * al(sizeof(uint32_t) * n) + 2 * al(sizeof(uint32_t) * G) +
+         al(sizeof(uint32_t) * nchunk) + al(sizeof(uint32_t) * std::max<int64_t>(nboot, 1) * n);
 }
 
 void dirac_job_bind(DiracJob &j, char *scratch, int *misc) {
   const int N = j.g->ndim;
   const int64_t nc = int64_t(1) << N;
   const int64_t G = grid_size(j.g);
+  const int64_t nchunk = (G + kScanChunk - 1) / kScanChunk;
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   j.cell = (uint32_t *)scratch;
   scratch += al(sizeof(uint32_t) * j.n);
   j.rh = (double *)scratch;
   scratch += al(sizeof(double) * N * j.n + sizeof(unsigned long long) * 2 * nc * j.n);
   j.counts = (uint32_t *)scratch;
-  (void)G;
+  scratch += al(sizeof(uint32_t) * (j.nboot + 1) * G);
+  j.pos = (uint32_t *)scratch;
+  scratch += al(sizeof(uint32_t) * j.n);
+  j.cell_sorted = (uint32_t *)scratch;
+  scratch += al(sizeof(uint32_t) * j.n);
+  j.cstart = (uint32_t *)scratch;
+  scratch += al(sizeof(uint32_t) * G);
+  j.cfill = (uint32_t *)scratch;
+  scratch += al(sizeof(uint32_t) * G);
+  j.csum = (uint32_t *)scratch;
+  scratch += al(sizeof(uint32_t) * nchunk);
+  j.mult = (uint32_t *)scratch;
   j.misc = misc;
 }
 
@@ -397,6 +602,39 @@ void dirac_job_phase_a(pkde_ctx *ctx, DiracJob &j, cudaStream_t st) {
     max_kernel<<<grid_blocks(ctx, nslots * G), kThreads, 0, st>>>(j.counts, nslots * G, maxc);
   }
   PKDE_CHECK_LAUNCH();
+  // samples in lower-cell order (counting sort from the identity counts), then each
+  // resample's draws as per-sample multiplicities in that order
+  const uint32_t *idc = j.counts + j.nboot * G;
+  const int64_t nchunk = (G + kScanChunk - 1) / kScanChunk;
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    cell_chunk_sum_kernel<<<(unsigned)nchunk, kThreads, 0, st>>>(idc, G, j.csum);
+  }
+  PKDE_CHECK_LAUNCH();
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    chunk_scan_kernel<<<1, 32, 0, st>>>(j.csum, nchunk);
+  }
+  PKDE_CHECK_LAUNCH();
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    cell_start_kernel<<<(unsigned)nchunk, kThreads, 0, st>>>(idc, G, j.csum, j.cstart, j.cfill);
+  }
+  PKDE_CHECK_LAUNCH();
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    cell_sort_kernel<<<grid_blocks(ctx, n), kThreads, 0, st>>>(j.cell, n, j.cstart, j.cfill, j.pos, j.cell_sorted);
+  }
+  PKDE_CHECK_LAUNCH();
+  if (j.nboot > 0) {
+    PKDE_CUDA_TRY(cudaMemsetAsync(j.mult, 0, sizeof(uint32_t) * j.nboot * n, st));
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+      mult_kernel<<<grid_blocks(ctx, j.nboot * n), kThreads, 0, st>>>(n, j.nboot, j.d_idx, j.seed, j.pos, j.mult,
+                                                                     misc);
+    }
+    PKDE_CHECK_LAUNCH();
+  }
 }
 
 // Phase B, given misc[0..1] read back: error check, fixed-point scales, quantised
@@ -432,8 +670,8 @@ void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_
   const int e_v = 62 - ex_v;
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
-    quantize_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(gd, j.rh, n, denom, e_m, e_v, qm,
-                                                                                     qv);
+    quantize_sorted_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(gd, j.rh, n, denom, e_m,
+                                                                                            e_v, j.pos, qm, qv);
   }
   PKDE_CHECK_LAUNCH();
   const double sm = std::ldexp(1.0, -e_m), sv = std::ldexp(1.0, -e_v);
@@ -442,8 +680,17 @@ void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_
   PKDE_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double2) * (2 * npairs + 1) * G, st));
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
-    weight_kernel<true><<<grid_blocks(ctx, nslots * n), kThreads, 0, st>>>(
-        j.cell, n, nslots, nboot, G, N, corner_off, j.d_idx, j.seed, qm, qv, acc, nullptr, npairs, j.misc);
+    const int blocks = grid_blocks(ctx, nslots * n);
+#define PKDE_WS(NN)                                                                                          \
+  weight_sorted_kernel<NN><<<blocks, kThreads, 0, st>>>(j.cell_sorted, n, nboot, G, corner_off, j.mult, qm, qv, acc, \
+                                                        npairs)
+    switch (N) {
+      case 1: PKDE_WS(1); break;
+      case 2: PKDE_WS(2); break;
+      case 3: PKDE_WS(3); break;
+      default: PKDE_WS(4); break;
+    }
+#undef PKDE_WS
   }
   PKDE_CHECK_LAUNCH();
   {

@@ -494,6 +494,9 @@ struct DiracJob {
   uint32_t *cell = nullptr;
   double *rh = nullptr;
   uint32_t *counts = nullptr;
+  uint32_t *pos = nullptr, *cell_sorted = nullptr;  // samples in lower-cell order
+  uint32_t *cstart = nullptr, *cfill = nullptr, *csum = nullptr;
+  uint32_t *mult = nullptr;  // nboot x n draws per sample (cell order)
   int *misc = nullptr;  // 256-byte device block
   int64_t corner_off_h[16] = {};
 };
