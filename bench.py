@@ -176,7 +176,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "batched", "served"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "batched", "batched-small", "served"])
     ap.add_argument("--rate", type=float, default=50.0, help="requests/s (--workload served)")
     ap.add_argument("--requests", type=int, default=64, help="requests (--workload served)")
     ap.add_argument("--lanes", type=int, default=2, help="serving lanes (--workload served)")
@@ -188,7 +188,7 @@ def main():
                     help="override the workload's bandwidth steps (small profiling runs only)")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
-    if args.workload == "batched":
+    if args.workload in ("batched", "batched-small"):
         return run_batched(args, world, rank, local, dist)
     if args.workload == "served":
         return run_served(args, world, rank, local, dist)
@@ -329,7 +329,7 @@ def main():
         dist.destroy_process_group()
 
 
-def batched_jobs(count, seed, device, torch):
+def batched_jobs(count, seed, device, torch, small=False):
     """The batched workload: `count` independent estimations, dims uniform in {1,2,3},
     samples log-uniform in [1e3, 1e6] from random 1-4 component Gaussian mixtures, grids
     256-4096 (1-D), 128^2-512^2 (2-D), 32^3-96^3 (3-D), 100 bandwidth steps, 32
@@ -338,7 +338,8 @@ def batched_jobs(count, seed, device, torch):
     import pkde_b200 as pk
     from pkde_b200 import workloads as W
     jobs = []
-    for e, m in enumerate(W.batched_mix(count=count, seed=seed)):
+    mix = W.batched_small_mix(count=count, seed=seed) if small else W.batched_mix(count=count, seed=seed)
+    for e, m in enumerate(mix):
         grid = pk.find_grid(m["data"], grid_dims=m["dims"])
         G = int(np.prod(grid.dims))
         host = np.ascontiguousarray(m["data"].T)
@@ -361,7 +362,8 @@ def run_batched(args, world, rank, local, dist):
     dev = torch.device("cuda", local)
     pk.load()
     pk.context(local)
-    jobs = batched_jobs(args.batch, 3 + rank, dev, torch)
+    small = args.workload == "batched-small"
+    jobs = batched_jobs(args.batch, 3 + rank, dev, torch, small=small)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
     units = sum(int(np.prod(j["grid"].dims)) * (j["n_steps"] + 1) for j in jobs)
@@ -459,8 +461,10 @@ def run_batched(args, world, rank, local, dist):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"batched: {len(jobs)} estimations per step, dims 1-3, n log-uniform 1e3-1e6, "
-                               "grids 256-4096 / 128^2-512^2 / 32^3-96^3, 101 bandwidths, B=32",
+        "config": {"workload": (f"batched-small: {len(jobs)} estimations per step, dims 1-2, n log-uniform 1e3-1e4, "
+                                "grids 256-1024 / 64^2-128^2, 101 bandwidths, B=32") if small else
+                               (f"batched: {len(jobs)} estimations per step, dims 1-3, n log-uniform 1e3-1e6, "
+                                "grids 256-4096 / 128^2-512^2 / 32^3-96^3, 101 bandwidths, B=32"),
                    "shapes": kinds, "estimations_per_s": est_per_s,
                    "plain_form_estimations_per_s": len(jobs) * world / (plain_ms / 1000.0),
                    "engine_one_at_a_time_estimations_per_s": len(jobs) * world / (engine_single_ms / 1000.0),

@@ -70,6 +70,7 @@ int pkde_destroy(pkde_ctx *ctx) {
   pkde::stop_server(ctx);  // finishes the queued requests first
   cudaDeviceSynchronize();
   for (auto &b : ctx->buf) b.release();
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
   delete ctx;
   return PKDE_OK;
 }

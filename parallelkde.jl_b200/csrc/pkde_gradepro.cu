@@ -15,8 +15,10 @@
 //   state    : f_prev1, f_prev2, minima (FP64), counters_low/over (u16), flags (u8),
 //              density (FP64), selected step (i32), final-step means (FP64).
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <limits>
+#include <thread>
 
 #include "pkde_internal.cuh"
 #include "pkde_step.cuh"
@@ -452,6 +454,51 @@ static void factor_tables(const pkde_grid *g, const Ladder &L, std::vector<doubl
   }
 }
 
+// The same tables written straight into fz/fw (S x tot each), steps [s0, s1).
+static void fill_factor_tables(const pkde_grid *g, const Ladder &L, const std::vector<int64_t> &axis_off, double *fz,
+                               double *fw, int64_t s0, int64_t s1) {
+  const int N = g->ndim;
+  const int64_t tot = axis_off[N];
+  const double two_pi = 6.283185307179586;
+  for (int64_t s = s0; s < s1; ++s) {
+    for (int j = 0; j < N; ++j) {
+      const int64_t n = g->dims[j];
+      const double mult = two_pi * ((1.0 / g->h[j]) / (double)n);
+      const double t = L.times[s * N + j];
+      const int64_t nneg = (n - 1) / 2 + 1;
+      for (int64_t m = 0; m < n; ++m) {
+        const double mm = (double)(m < nneg ? m : m - n);
+        const double kt = (mm * mult) * t;
+        const double pv = std::exp(-0.5 * (kt * kt));
+        fz[s * tot + axis_off[j] + m] = pv;
+        fw[s * tot + axis_off[j] + m] = std::sqrt(pv);
+      }
+    }
+  }
+}
+
+static void axis_offsets(const pkde_grid *g, std::vector<int64_t> &axis_off) {
+  int64_t tot = 0;
+  axis_off.assign(g->ndim + 1, 0);
+  for (int j = 0; j < g->ndim; ++j) {
+    axis_off[j] = tot;
+    tot += g->dims[j];
+  }
+  axis_off[g->ndim] = tot;
+}
+
+// Page-locked staging buffer of the context (grow-only), for asynchronous uploads.
+static void *pinned_staging(pkde_ctx *ctx, size_t bytes) {
+  if (bytes > ctx->pinned_bytes) {
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    PKDE_CUDA_TRY(cudaMallocHost(&ctx->pinned, bytes));
+    ctx->pinned_bytes = bytes;
+  }
+  return ctx->pinned;
+}
+
 template <class K>
 static void set_smem(K kernel, size_t bytes) {
   PKDE_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -478,7 +525,6 @@ struct Plan {
   int64_t G, B, npairs;
   StepPath path;
   Ladder L;
-  std::vector<double> fz, fw;
   std::vector<int64_t> aoff;
   int64_t tot;
   // device buffers (in the call's arena)
@@ -630,10 +676,6 @@ static void run_generic(pkde_ctx *ctx, Plan &P, cudaStream_t st) {
   }
 }
 
-static void make_plan_tables(Plan &P) {
-  factor_tables(P.g, P.L, P.fz, P.fw, P.aoff);
-  P.tot = P.aoff[P.N];
-}
 
 // The :gradepro estimation of `count` independent sample sets on one stream: each phase
 // runs for every estimation before the next phase starts, so the whole call has one
@@ -680,7 +722,8 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
     for (int j = 0; j < P.N; ++j)
       if (!std::isnan(ests[e].p->bw_final[j])) bw[j] = ests[e].p->bw_final[j];
     P.L = make_ladder(ests[e].p, bw, ests[e].n);
-    make_plan_tables(P);
+    axis_offsets(P.g, P.aoff);
+    P.tot = P.aoff[P.N];
     P.path = steps1d_ok(P.g) ? StepPath::Steps1D : (engine_ok(P.g) ? StepPath::Engine : StepPath::Generic);
     if (ctx->step_path == PKDE_STEPS_PER_STEP_LAUNCH) P.path = StepPath::Generic;
     tables_bytes += al256(sizeof(double) * 2 * P.L.S * P.tot);
@@ -708,15 +751,14 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
     ensure(ctx, BUF_SCRATCH, generic_scr);
     ensure(ctx, BUF_WELFORD, generic_wel);
   }
-  std::vector<char> htab(tables_bytes);
+  std::vector<size_t> toffs(count);
   size_t toff = 0;
   for (int e = 0; e < count; ++e) {
     Plan &P = plans[e];
     const int64_t S = P.L.S;
     P.misc = (int *)(base + 256 * (size_t)e);
     P.tables = (double *)(base + off_tables + toff);
-    std::memcpy(htab.data() + toff, P.fz.data(), sizeof(double) * S * P.tot);
-    std::memcpy(htab.data() + toff + sizeof(double) * S * P.tot, P.fw.data(), sizeof(double) * S * P.tot);
+    toffs[e] = toff;
     toff += al256(sizeof(double) * 2 * S * P.tot);
     char *q = base + off[e];
     P.spectra = (double2 *)q;
@@ -738,10 +780,36 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
     P.job.paired_out = P.spectra;
     dirac_job_bind(P.job, P.bin_scratch, P.misc);
   }
-  if (tables_bytes)
-    PKDE_CUDA_TRY(cudaMemcpyAsync(base + off_tables, htab.data(), tables_bytes, cudaMemcpyHostToDevice, st));
-  // ---- binning: phase A for all, one read-back, phase B for all
+  // ---- binning: phase A for all (queued first, so that the host work below overlaps it)
   for (int e = 0; e < count; ++e) dirac_job_phase_a(ctx, plans[e].job, st);
+  // ---- propagation factor tables: host threads into page-locked memory, one async upload
+  if (tables_bytes) {
+    char *hp = (char *)pinned_staging(ctx, tables_bytes);
+    struct Chunk {
+      int e;
+      int64_t s0, s1;
+    };
+    std::vector<Chunk> chunks;
+    for (int e = 0; e < count; ++e) {
+      const int64_t S = plans[e].L.S, per = std::max<int64_t>(1, (int64_t)(1 << 16) / std::max<int64_t>(1, plans[e].tot));
+      for (int64_t s0 = 0; s0 < S; s0 += per) chunks.push_back({e, s0, std::min(S, s0 + per)});
+    }
+    const int nth = (int)std::min<size_t>(chunks.size(), std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+    std::atomic<size_t> next{0};
+    auto work = [&] {
+      for (size_t k; (k = next.fetch_add(1)) < chunks.size();) {
+        const Chunk &c = chunks[k];
+        const Plan &P = plans[c.e];
+        double *fz = (double *)(hp + toffs[c.e]);
+        fill_factor_tables(P.g, P.L, P.aoff, fz, fz + P.L.S * P.tot, c.s0, c.s1);
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nth; ++i) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    PKDE_CUDA_TRY(cudaMemcpyAsync(base + off_tables, hp, tables_bytes, cudaMemcpyHostToDevice, st));
+  }
   std::vector<int> hmisc(64 * (size_t)count);
   PKDE_CUDA_TRY(cudaMemcpyAsync(hmisc.data(), base, 256 * (size_t)count, cudaMemcpyDeviceToHost, st));
   PKDE_CUDA_TRY(cudaStreamSynchronize(st));

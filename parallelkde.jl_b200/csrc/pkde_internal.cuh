@@ -102,6 +102,9 @@ struct pkde_ctx {
   bool autotune = true;
   bool tune_loaded = false;
   std::map<std::string, std::array<int, 3>> tune;
+  // page-locked staging buffer for asynchronous uploads (grow-only)
+  void *pinned = nullptr;
+  size_t pinned_bytes = 0;
   // serving (pkde_serve.cu): created on the first pkde_submit
   void *server = nullptr;
   int serve_lanes = 2;

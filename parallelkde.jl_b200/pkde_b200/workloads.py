@@ -108,3 +108,20 @@ def served_mix(count=48, seed=4, n_range=(1e3, 4e6), n_steps=100, n_boot=32):
             g = (s, s, s, s)
         out.append(dict(data=random_mixture(ndim, n, rng), dims=g, n_steps=n_steps, n_bootstraps=n_boot))
     return out
+
+
+def batched_small_mix(count=256, seed=5, n_range=(1e3, 1e4), n_steps=100, n_boot=32):
+    """Small estimations, where one estimation alone cannot fill the GPU: dims 1 or 2,
+    samples log-uniform in n_range, grids 256-1024 (1-D) and 64^2-128^2 (2-D)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        ndim = int(rng.integers(1, 3))
+        n = int(round(math.exp(rng.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+        if ndim == 1:
+            g = (int(2 ** rng.integers(8, 11)),)
+        else:
+            s = int(rng.choice([64, 96, 128]))
+            g = (s, s)
+        out.append(dict(data=random_mixture(ndim, n, rng), dims=g, n_steps=n_steps, n_bootstraps=n_boot))
+    return out
