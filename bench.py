@@ -236,12 +236,13 @@ def main():
 
     for w in range(args.warmup):
         one(1000 + w)
-    # timed region: K estimations, samples resident in HBM; profiling events on
+    # timed region: K estimations, samples resident in HBM; events around the step-engine
+    # launches only (the per-phase breakdown comes from one profiled estimation afterwards)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     _lib.get_stats(local, reset=True)
-    _lib.set_profiling(True, local)
+    _lib.set_profiling(_lib.PKDE_PROFILE_STEPS, local)
     clocks = Clocks(local)
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -257,7 +258,7 @@ def main():
     ev1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    _lib.set_profiling(False, local)
+    _lib.set_profiling(_lib.PKDE_PROFILE_OFF, local)
     stats = _lib.get_stats(local, reset=True)
     elapsed_ms = ev0.elapsed_time(ev1)
     lat_ms = sorted(a.elapsed_time(b) for a, b in lat)
@@ -276,15 +277,26 @@ def main():
         e0 = time.perf_counter()
         ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev2.record(stream)
+        e2e_walls = []
         for k in range(args.steps):
+            tk = time.perf_counter()
             pk.estimate_density(est, "gradepro", n_bootstraps=kw["n_bootstraps"], n_steps=kw["n_steps"],
                                 seed=multi.estimation_seed(rank, k), device_id=local)
             pk.get_density(est)
+            e2e_walls.append((time.perf_counter() - tk) * 1000.0)
         ev3.record(stream)
         torch.cuda.synchronize()
         e2e_ms = max(ev2.elapsed_time(ev3), (time.perf_counter() - e0) * 1000.0)
         e2e_ms = multi.max_over_ranks(e2e_ms, dist, dev)
         e2e_value = units / (e2e_ms / 1000.0)
+
+    # per-phase breakdown: one more estimation with every launch timed (not in any timed region)
+    _lib.get_stats(local, reset=True)
+    _lib.set_profiling(_lib.PKDE_PROFILE_ALL, local)
+    one(4242)
+    torch.cuda.synchronize()
+    _lib.set_profiling(_lib.PKDE_PROFILE_OFF, local)
+    pstats = _lib.get_stats(local, reset=True)
 
     # roofline of the per-bandwidth-step pipeline: FP64 spectra (2 bootstraps' means or
     # second moments per complex array, plus the full-sample means) read once per step:
@@ -296,7 +308,7 @@ def main():
     step_launches = sum(stats["phase_launches"][p] for p in step_phases) / args.steps
     alg_bytes = 16.0 * (B + 1) * G * S
     achieved = alg_bytes / (step_ms / 1000.0) / 1e9 if step_ms > 0 else None
-    dominant = max(stats["phase_ms"], key=lambda p: stats["phase_ms"][p])
+    dominant = max(pstats["phase_ms"], key=lambda p: pstats["phase_ms"][p])
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -307,7 +319,8 @@ def main():
                    "l2": "inputs (spectra 16(B+1)G bytes) larger than the 126 MB L2",
                    "parallelism": f"independent estimations per rank x{world}"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n * N * 8),
-                "d2h_bytes_per_step": int(G * 12)},
+                "d2h_bytes_per_step": int(G * 12),
+                "wall_ms_per_step": [round(v, 2) for v in e2e_walls] if e2e_value else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "traffic": measured_traffic(args.workload) if not args.bandwidth_steps else None,
@@ -315,7 +328,7 @@ def main():
                      "kernel": "engine_kernel (persistent step engine: all bandwidth steps, one launch)",
                      "peak_source": peak_kind, "step_ms_per_estimation": step_ms,
                      "launches_per_estimation": step_launches},
-        "phase_ms_per_estimation": {p: v / args.steps for p, v in stats["phase_ms"].items()},
+        "phase_ms_per_estimation": dict(pstats["phase_ms"]),
         "dominant_phase": dominant,
         "gpu_launches": stats["launches"],
         "clocks": clk,
@@ -378,7 +391,7 @@ def run_batched(args, world, rank, local, dist):
     if dist:
         dist.barrier()
     _lib.get_stats(local, reset=True)
-    _lib.set_profiling(True, local)
+    _lib.set_profiling(_lib.PKDE_PROFILE_STEPS, local)
     clocks = Clocks(local)
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -394,8 +407,14 @@ def run_batched(args, world, rank, local, dist):
     ev1.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    _lib.set_profiling(False, local)
+    _lib.set_profiling(_lib.PKDE_PROFILE_OFF, local)
     stats = _lib.get_stats(local, reset=True)
+    # per-phase breakdown from one more batch with every launch timed (untimed)
+    _lib.set_profiling(_lib.PKDE_PROFILE_ALL, local)
+    batch()
+    torch.cuda.synchronize()
+    _lib.set_profiling(_lib.PKDE_PROFILE_OFF, local)
+    pstats = _lib.get_stats(local, reset=True)
     t_max = multi.max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     lat_ms = sorted(a.elapsed_time(b) for a, b in lat)
     value = units * args.steps * world / (t_max / 1000.0)
@@ -477,7 +496,7 @@ def run_batched(args, world, rank, local, dist):
                      "frac": (achieved / peak) if achieved else None, "traffic": None,
                      "kernel": "engine_kernel (all N-D estimations of the batch in one launch)",
                      "peak_source": peak_kind},
-        "phase_ms_per_step": {p: v / args.steps for p, v in stats["phase_ms"].items()},
+        "phase_ms_per_step": dict(pstats["phase_ms"]),
         "gpu_launches": stats["launches"],
         "clocks": clk,
     }

@@ -251,8 +251,15 @@ int pkde_set_autotune(pkde_ctx *ctx, int enable);
 
 /* Launch accounting and per-phase device time, for tracing and the roofline report.
  * No counterpart in the reference, which has no tracing.
- * When enabled, every kernel the context launches is bracketed by CUDA events on its
- * stream and its elapsed time is added to its phase when the call synchronises. */
+ * pkde_set_profiling levels: PKDE_PROFILE_ALL brackets every kernel the context
+ * launches with CUDA events on its stream and adds its elapsed time to its phase when
+ * the call synchronises; PKDE_PROFILE_STEPS brackets only the bandwidth-step phases
+ * (2..4), two events per step-engine launch, so that timing a whole call is not
+ * slowed by events between short launches; PKDE_PROFILE_OFF brackets nothing.  Launch
+ * counts are kept at every level.  Other levels return PKDE_EINVAL. */
+#define PKDE_PROFILE_OFF 0
+#define PKDE_PROFILE_ALL 1
+#define PKDE_PROFILE_STEPS 2
 #define PKDE_NPHASES 6
 typedef enum pkde_phase {
   PKDE_PHASE_BINNING = 0,      /* binning + fixed-point conversion */

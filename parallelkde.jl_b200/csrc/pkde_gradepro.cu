@@ -1115,7 +1115,8 @@ int pkde_set_autotune(pkde_ctx *ctx, int enable) {
 
 int pkde_set_profiling(pkde_ctx *ctx, int enable) {
   if (!ctx) return PKDE_EINVAL;
-  ctx->profiling = enable != 0;
+  if (enable < PKDE_PROFILE_OFF || enable > PKDE_PROFILE_STEPS) return PKDE_EINVAL;
+  ctx->profiling = enable;
   return PKDE_OK;
 }
 

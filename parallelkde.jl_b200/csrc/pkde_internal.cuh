@@ -96,7 +96,7 @@ struct pkde_ctx {
   int sm_count = 0;
   size_t smem_optin = 0;
   // tracing (pkde_set_profiling / pkde_get_stats)
-  bool profiling = false;
+  int profiling = PKDE_PROFILE_OFF;
   int step_path = 0;  // PKDE_STEPS_AUTO / PKDE_STEPS_PER_STEP_LAUNCH
   // engine schedule per shape (pkde_set_autotune): key -> {slot MB, tiles per item, delay}
   bool autotune = true;
@@ -141,7 +141,8 @@ struct Trace {
   Trace(pkde_ctx *c, int p, cudaStream_t s) : ctx(c), phase(p), st(s) {
     ctx->launches++;
     ctx->phase_launches[p]++;
-    if (ctx->profiling) {
+    if (ctx->profiling == PKDE_PROFILE_ALL ||
+        (ctx->profiling == PKDE_PROFILE_STEPS && p >= PKDE_PHASE_STEP_FFT && p <= PKDE_PHASE_STEP_MEANS)) {
       a = pooled_event(ctx);
       cudaEventRecord(a, st);
     }

@@ -158,8 +158,14 @@ def make_params(grid_struct, n_bootstraps=100, n_steps=None, bw_step=None, bw_fi
     return p
 
 
+PKDE_PROFILE_OFF, PKDE_PROFILE_ALL, PKDE_PROFILE_STEPS = 0, 1, 2
+
+
 def set_profiling(enable, device=0):
-    load().pkde_set_profiling(context(device), int(bool(enable)))
+    """True / PKDE_PROFILE_ALL: time every launch per phase; PKDE_PROFILE_STEPS: only
+    the bandwidth-step phases; False / PKDE_PROFILE_OFF: launch counts only."""
+    ctx = context(device)
+    check(load().pkde_set_profiling(ctx, int(enable)), ctx)
 
 
 PKDE_STEPS_AUTO, PKDE_STEPS_PER_STEP_LAUNCH = 0, 1

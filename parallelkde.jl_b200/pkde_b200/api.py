@@ -56,9 +56,20 @@ class KDE:
         import torch
         t = torch.empty(self.samples.shape, dtype=torch.float64, pin_memory=True)
         t.numpy()[...] = self.samples
-        self._pinned = t
+        dp = torch.empty(self.density.shape, dtype=torch.float64, pin_memory=True)
+        dp.numpy()[...] = self.density
+        self._pinned = (t, dp)
         self.samples = t.numpy()
+        self.density = dp.numpy()
         return self
+
+    def density_out(self):
+        """A flat FP64 view of ``density`` the library can write into directly, or None
+        when ``density`` was replaced by an array of another layout."""
+        d = self.density
+        if isinstance(d, np.ndarray) and d.dtype == np.float64 and d.flags.c_contiguous and d.flags.writeable:
+            return d.reshape(-1)
+        return None
 
 
 def _as_samples(data):
@@ -254,7 +265,8 @@ class GradeProEstimator(AbstractEstimator):
         ctx = context(self.device_id)
         lib = load()
         G = int(np.prod(self.grid.dims))
-        dens = np.empty(G, dtype=np.float64)
+        direct = kde.density_out()
+        dens = direct if direct is not None and direct.size == G else np.empty(G, dtype=np.float64)
         sel = np.empty(G, dtype=np.int32)
         data_t = kde.samples  # (n, N) C-contiguous == N x n column-major
         flags, idx = 0, self.idx
@@ -267,7 +279,8 @@ class GradeProEstimator(AbstractEstimator):
                                         ptr(idx), int(self.seed) & (2**64 - 1), ptr(dens), ptr(sel), flags,
                                         self.stream)
         check(rc, ctx)
-        kde.density[...] = dens.reshape(kde.density.shape)
+        if dens is not direct:
+            kde.density[...] = dens.reshape(kde.density.shape)
         self.selected_step = sel.reshape(kde.density.shape)
 
 
@@ -305,14 +318,16 @@ class RoTEstimator(AbstractEstimator):
         ctx = context(self.device_id)
         lib = load()
         G = int(np.prod(self.grid.dims))
-        dens = np.empty(G, dtype=np.float64)
+        direct = kde.density_out()
+        dens = direct if direct is not None and direct.size == G else np.empty(G, dtype=np.float64)
         data_t = kde.samples
         flags = 0 if isinstance(data_t, np.ndarray) else _lib.PKDE_DEVICE_INPUT
         gs = make_grid_struct(self.grid.lo, self.grid.hi, self.grid.h, self.grid.dims)
         rc = lib.pkde_rot_estimate(ctx, ctypes.byref(gs), self.RULES[self.rule], ptr(data_t), data_t.shape[0],
                                    ptr(dens), flags, self.stream)
         check(rc, ctx)
-        kde.density[...] = dens.reshape(kde.density.shape)
+        if dens is not direct:
+            kde.density[...] = dens.reshape(kde.density.shape)
 
 
 add_estimator("rot", RoTEstimator)

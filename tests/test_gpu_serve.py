@@ -75,7 +75,7 @@ def test_served_bad_request_fails_alone(pk):
     results = [srv.wait(t) for t in tickets]
     assert results[3]["status"] == 1 and "beyond grid" in results[3]["message"]
     for i in (0, 1, 2, 4, 5):
-        assert results[i]["status"] == 0
+        assert results[i]["status"] == 0, results[i]["message"]
         d, s = _alone(reqs[i])
         assert np.array_equal(results[i]["density"].reshape(-1), d)
     with pytest.raises(pk.ArgumentError, match="unknown ticket"):
