@@ -109,13 +109,13 @@ void fft_axis(pkde_ctx *ctx, const LineSet &ls, const double2 *in, double2 *out,
   const double s0 = scal ? scal[0] : 1.0;
   const double s1 = (scal && nfac > 1) ? scal[1] : s0;
   if (dir < 0) {
-    PKDE_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_dynamic_smem(ctx, fft_axis_kernel<-1>, smem);
     {
       ::pkde::Trace _tr(ctx, phase, st);
       fft_axis_kernel<-1><<<(unsigned)blocks, kFftThreads, smem, st>>>(in, out, ls, plan, tw, f0, f1, s0, s1, nfac, tl, pitch);
     }
   } else {
-    PKDE_CUDA_TRY(cudaFuncSetAttribute(fft_axis_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    allow_dynamic_smem(ctx, fft_axis_kernel<1>, smem);
     {
       ::pkde::Trace _tr(ctx, phase, st);
       fft_axis_kernel<1><<<(unsigned)blocks, kFftThreads, smem, st>>>(in, out, ls, plan, tw, f0, f1, s0, s1, nfac, tl, pitch);

@@ -499,11 +499,6 @@ static void *pinned_staging(pkde_ctx *ctx, size_t bytes) {
   return ctx->pinned;
 }
 
-template <class K>
-static void set_smem(K kernel, size_t bytes) {
-  PKDE_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-}
-
 // One estimation of a call (device pointers).
 struct Estimation {
   const pkde_gradepro_params *p;
@@ -594,7 +589,7 @@ static void run_generic(pkde_ctx *ctx, Plan &P, cudaStream_t st) {
                         double cw) {
 #define PKDE_VMR_CASE(P)                                                                                   \
   if (ppt_needed <= P) {                                                                                   \
-    set_smem(vmr_axis1_kernel<P>, smem);                                                                   \
+    allow_dynamic_smem(ctx, vmr_axis1_kernel<P>, smem);                                                               \
     { \
       ::pkde::Trace _tr(ctx, PKDE_PHASE_STEP_VMR, st); \
       vmr_axis1_kernel<P><<<fblocks, kThreads, smem, st>>>(in, np, b0, (int)B, n1, rows, plan1, tw1, fz1,   \
@@ -612,7 +607,7 @@ static void run_generic(pkde_ctx *ctx, Plan &P, cudaStream_t st) {
   auto launch_means = [&](const double2 *in, const double *fz1, double cz, int64_t s) {
 #define PKDE_MEANS_CASE(P)                                                                                    \
   if (ppt_needed <= P) {                                                                                      \
-    set_smem(means_converge_kernel<P>, smem);                                                                 \
+    allow_dynamic_smem(ctx, means_converge_kernel<P>, smem);                                                             \
     { \
       ::pkde::Trace _tr(ctx, PKDE_PHASE_STEP_MEANS, st); \
       means_converge_kernel<P><<<fblocks, kThreads, smem, st>>>(in, n1, rows, plan1, tw1, fz1, cz, wm2,        \

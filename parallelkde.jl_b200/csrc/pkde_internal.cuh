@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <array>
 #include <map>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -155,6 +156,38 @@ struct Trace {
     }
   }
 };
+// Dynamic shared memory above 48 KB must be allowed per kernel with cudaFuncSetAttribute,
+// which sets a property of the kernel for the whole process, not of one launch.  Serving
+// lanes launch from several host threads: if each call set the size its own launch
+// needs, one thread could lower the limit between another thread's setting and its
+// launch, and that launch would fail.  So the limit only grows (under a lock, per kernel
+// and device): it is raised to a launch's need when that need is larger, and never
+// lowered, so every launch finds at least what it asked for.  A need beyond what the
+// device allows next to the kernel's static shared memory is refused.
+template <class K>
+inline void allow_dynamic_smem(pkde_ctx *ctx, K kernel, size_t bytes) {
+  struct Limit {
+    size_t cap, set;
+  };
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, Limit> limits;
+  const void *fn = reinterpret_cast<const void *>(kernel);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = limits.find(std::make_pair(fn, ctx->device));
+  if (it == limits.end()) {
+    cudaFuncAttributes fa;
+    PKDE_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
+    const size_t cap = ctx->smem_optin > fa.sharedSizeBytes ? ctx->smem_optin - fa.sharedSizeBytes : 0;
+    it = limits.emplace(std::make_pair(fn, ctx->device), Limit{cap, 0}).first;
+  }
+  Limit &L = it->second;
+  if (bytes > L.cap) throw Error{PKDE_EUNSUPPORTED, "a kernel needs more shared memory than an SM offers"};
+  if (bytes > L.set) {
+    PKDE_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    L.set = bytes;
+  }
+}
+
 // Fold finished event pairs into phase_ms (call after the stream synchronised).
 inline void collect_trace(pkde_ctx *ctx) {
   for (auto &p : ctx->pending) {

@@ -270,7 +270,7 @@ void launch_axis(pkde_ctx *ctx, const LineSet &ls, const double2 *in, double2 *o
                  const double *scal, int nfac, cudaStream_t st) {
   using P = Pow2<LOGN>;
   const size_t smem = tile_smem_bytes<LOGN>();
-  PKDE_CUDA_TRY(cudaFuncSetAttribute(axis_pass_pow2_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(ctx, axis_pass_pow2_kernel<LOGN>, smem);
   const double2 *tw = stage_twiddles_device(ctx, LOGN);
   const int64_t blocks = ls.nlines() / P::NL;
   {
@@ -288,7 +288,7 @@ void launch_vmr(pkde_ctx *ctx, const double2 *in, int npairs, int b0, int nboot,
                 cudaStream_t st) {
   using P = Pow2<LOGN>;
   const size_t smem = tile_smem_bytes<LOGN>() + sizeof(double2) * 8 * P::THREADS;
-  PKDE_CUDA_TRY(cudaFuncSetAttribute(vmr_pass_pow2_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(ctx, vmr_pass_pow2_kernel<LOGN>, smem);
   const double2 *tw = stage_twiddles_device(ctx, LOGN);
   {
     Trace tr(ctx, PKDE_PHASE_STEP_VMR, st);
@@ -304,7 +304,7 @@ void launch_means(pkde_ctx *ctx, const double2 *in, int64_t rows, const double *
                   int64_t steps_over, const StepState &cs, int step, cudaStream_t st) {
   using P = Pow2<LOGN>;
   const size_t smem = tile_smem_bytes<LOGN>();
-  PKDE_CUDA_TRY(cudaFuncSetAttribute(means_pass_pow2_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(ctx, means_pass_pow2_kernel<LOGN>, smem);
   const double2 *tw = stage_twiddles_device(ctx, LOGN);
   {
     Trace tr(ctx, PKDE_PHASE_STEP_MEANS, st);
@@ -327,7 +327,7 @@ void launch_steps1d(pkde_ctx *ctx, const double2 *spectra, int npairs, int nboot
                     const double *vscale, double *f_out, double *mu_out, cudaStream_t st) {
   using P = Pow2<LOGN, 1>;
   const size_t smem = sizeof(double2) * ((size_t)P::TILE + P::TWSIZE);
-  PKDE_CUDA_TRY(cudaFuncSetAttribute(steps1d_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(ctx, steps1d_kernel<LOGN>, smem);
   const double2 *tw = stage_twiddles_device(ctx, LOGN);
   {
     Trace tr(ctx, PKDE_PHASE_STEP_VMR, st);
