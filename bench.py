@@ -50,10 +50,10 @@ def measured_traffic(workload):
     engine launch, from the committed ncu summary of that kernel (profiles/); None if
     there is no capture for this workload."""
     import re
-    p = os.path.join(REPO, "profiles", "engine_kernel_c2_ncu.md")
-    if workload != "c2" or not os.path.exists(p):
+    p = os.path.join(REPO, "profiles", f"engine_kernel_{workload}_ncu.md")
+    if not os.path.exists(p):
         return None
-    m = re.search(r"dram_bytes_per_launch_full_c2:\s*([0-9.eE+]+)", open(p).read())
+    m = re.search(rf"dram_bytes_per_launch_full_{workload}:\s*([0-9.eE+]+)", open(p).read())
     return float(m.group(1)) if m else None
 
 

@@ -182,3 +182,36 @@ def test_autotune_keeps_results_and_caches(pk, tmp_path, monkeypatch):
     assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
     lines = cache.read_text().split()
     assert lines and lines[0] == "2x64x48:p5" and len(lines) == 4
+
+
+@pytest.mark.parametrize("dims", [(64, 48), (16, 32, 16), (24, 20, 12)])
+def test_engine_schedules_keep_results(pk, monkeypatch, dims):
+    """Every schedule the autotuner may pick (pipeline delay 1..4, ring-slot sizes from one
+    pair per group up to all pairs, tiles per item) gives the same densities and steps."""
+    import ctypes
+    from pkde_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(len(dims))
+    x = rng.standard_normal((len(dims), 5000))
+    grid = pk.find_grid(x, grid_dims=dims)
+    p = _lib.make_params(_lib.make_grid_struct(grid.lo, grid.hi, grid.h, grid.dims), 10, 24)
+    data = np.ascontiguousarray(x.T)
+    G = int(np.prod(dims))
+    ctx = ctypes.c_void_p()
+    assert lib.pkde_create(ctypes.byref(ctx), 0) == 0
+    outs = []
+    try:
+        assert lib.pkde_set_autotune(ctx, 0) == 0
+        for delay, slot_mb, tpi in ((2, 32, 2), (1, 1, 1), (1, 32, 4), (3, 1, 8), (4, 2, 2)):
+            monkeypatch.setenv("PKDE_ENGINE_DELAY", str(delay))
+            monkeypatch.setenv("PKDE_ENGINE_SLOT_MB", str(slot_mb))
+            monkeypatch.setenv("PKDE_ENGINE_TPI", str(tpi))
+            d, s = np.empty(G), np.empty(G, dtype=np.int32)
+            rc = lib.pkde_gradepro_estimate(ctx, ctypes.byref(p), _lib.ptr(data), data.shape[0], None, 5, _lib.ptr(d),
+                                            _lib.ptr(s), 0, None)
+            _lib.check(rc, ctx)
+            outs.append((d, s))
+    finally:
+        lib.pkde_destroy(ctx)
+    for d, s in outs[1:]:
+        assert np.array_equal(d, outs[0][0]) and np.array_equal(s, outs[0][1])
