@@ -242,11 +242,15 @@ int pkde_set_step_path(pkde_ctx *ctx, int path);
 
 /* Autotuning of the step engine's schedule per shape (grid dimensions and bootstrap
  * pairs): the first estimation of a new shape times trial runs over its first 16
- * bandwidth steps for ring-slot sizes 8..64 MB, 1..8 tiles per work item and pipeline
- * delays 2..4, and keeps the fastest for the context (and, when the environment
- * variable PKDE_TUNE_CACHE names a file, appends it there and reads it back in later
- * processes).  The schedule never changes results, only time.  On by default; 0 uses
- * the fixed defaults (32 MB, 2 or 8 tiles, delay 2).  No counterpart in the reference. */
+ * bandwidth steps for ring-slot sizes 8..64 MB, slots holding half or all of the
+ * bootstrap pairs where those are larger (while the ring stays within an eighth of the
+ * free device memory; the context keeps the largest ring it tried), 1..8 tiles per
+ * work item and pipeline delays 2..4, and keeps the fastest for the context (and, when
+ * the environment variable PKDE_TUNE_CACHE names a file, appends it there and reads it
+ * back in later processes).  A batch whose tuned rings together would not fit in half
+ * of the free memory runs with slots of at most 64 MB.  The schedule never changes
+ * results, only time.  On by default; 0 uses the fixed defaults (32 MB, 2 or 8 tiles,
+ * delay 2).  No counterpart in the reference. */
 int pkde_set_autotune(pkde_ctx *ctx, int enable);
 
 /* Launch accounting and per-phase device time, for tracing and the roofline report.

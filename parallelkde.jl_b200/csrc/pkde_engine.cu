@@ -1217,7 +1217,7 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
   // the state region doubles as the second exchange buffer of the register-FFT axis passes
   const size_t state_elems = std::max<size_t>(max_reg_tile, 8 * kEngineThreads);
   const size_t smem = sizeof(double2) * (max_tile + state_elems + max_tw);
-  PKDE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  allow_dynamic_smem(ctx, kern, smem);
   int per_sm = 0;
   PKDE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kEngineThreads, smem));
   if (per_sm < 1) throw Error{PKDE_EUNSUPPORTED, "engine kernel does not fit on an SM"};
@@ -1234,6 +1234,11 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
 }
 
 void run_engine(pkde_ctx *ctx, const EngineArgs &A, cudaStream_t st) { run_engine_batch(ctx, &A, 1, st); }
+
+size_t engine_ring_bytes(const EngineArgs &A) {
+  const EngineEst E = describe(A);
+  return sizeof(double2) * (size_t)E.Q * (size_t)E.slot_elems;
+}
 
 // ---------------------------------------------------------------- autotuning
 // Key of a shape: grid dimensions and pairs of bootstraps (the schedule depends on
@@ -1279,6 +1284,33 @@ void autotune_engine(pkde_ctx *ctx, EngineArgs &A, cudaStream_t st) {
     std::vector<std::array<int, 3>> cand;
     for (int slot : {8, 16, 32, 64})
       for (int tpi : {1, 2, 4, 8}) cand.push_back({slot, tpi, 2});
+    // Wide groups: ring slots holding half or all of the bootstrap pairs.  With all pairs in
+    // one group a step has a single pair batch, so the final pass reads and writes the
+    // per-point Welford state once per step and no group waits for the previous one
+    // (measured: 512 x 512 / B = 64 engine 57.1 -> 53.2 ms, 128^3 / B = 32 252 -> 207 ms).
+    // Only where the slot exceeds the narrow sizes above and the ring (at the largest delay
+    // tried) stays within an eighth of the free device memory.
+    size_t freeb = 0, totalb = 0;
+    PKDE_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
+    const size_t budget = freeb / 8;
+    auto ring_fits = [&](const std::array<int, 3> &c) {
+      EngineArgs R = A;
+      R.tune_slot_mb = c[0];
+      R.tune_tpi = c[1];
+      R.tune_delay = c[2];
+      return engine_ring_bytes(R) <= budget;
+    };
+    if (ctx->tune_wide) {
+      const int64_t pair_bytes = (int64_t)sizeof(double2) * 2 * grid_size(A.grid);
+      int last_mb = 0;
+      for (int gg : {(A.npairs + 1) / 2, A.npairs}) {
+        const int64_t mb = (gg * pair_bytes + (1 << 20) - 1) >> 20;
+        if (mb <= kNarrowSlotMB || mb == last_mb || mb > (1 << 30)) continue;
+        last_mb = (int)mb;
+        for (int tpi : {2, 4, 8})
+          if (ring_fits({(int)mb, tpi, 4})) cand.push_back({(int)mb, tpi, 2});
+      }
+    }
     cudaEvent_t e0, e1;
     PKDE_CUDA_TRY(cudaEventCreate(&e0));
     PKDE_CUDA_TRY(cudaEventCreate(&e1));

@@ -881,8 +881,26 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
   {
     std::vector<EngineArgs> lean, wide;
     for (const EngineArgs &A : eng) (engine_register_only(A.grid) ? lean : wide).push_back(A);
-    if (!lean.empty()) run_engine_batch(ctx, lean.data(), (int)lean.size(), st);
-    if (!wide.empty()) run_engine_batch(ctx, wide.data(), (int)wide.size(), st);
+    // Schedules are tuned per shape, one estimation at a time; a launch of many estimations
+    // whose tuned ring slots are wide could need more memory than is free, so then every
+    // slot of that launch is narrowed (the schedule changes time, never results).
+    auto fit = [&](std::vector<EngineArgs> &v) {
+      size_t need = 0;
+      for (const EngineArgs &A : v) need += engine_ring_bytes(A);
+      size_t freeb = 0, totalb = 0;
+      PKDE_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
+      if (need <= (freeb + ctx->buf[BUF_ENGINE].bytes) / 2) return;
+      for (EngineArgs &A : v)
+        if (A.tune_slot_mb > kNarrowSlotMB) A.tune_slot_mb = kNarrowSlotMB;
+    };
+    if (!lean.empty()) {
+      fit(lean);
+      run_engine_batch(ctx, lean.data(), (int)lean.size(), st);
+    }
+    if (!wide.empty()) {
+      fit(wide);
+      run_engine_batch(ctx, wide.data(), (int)wide.size(), st);
+    }
   }
   // ---- replace_nans! and outputs
   for (int e = 0; e < count; ++e) {

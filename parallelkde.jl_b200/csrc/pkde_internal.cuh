@@ -34,7 +34,16 @@ struct Error {
     }                                                                                           \
   } while (0)
 
-#define PKDE_CHECK_LAUNCH() PKDE_CUDA_TRY(cudaGetLastError())
+// After a kernel launch: the launch's error, with the launching source line.
+#define PKDE_STR2(x) #x
+#define PKDE_STR(x) PKDE_STR2(x)
+#define PKDE_CHECK_LAUNCH()                                                                                \
+  do {                                                                                                     \
+    cudaError_t _e = cudaGetLastError();                                                                   \
+    if (_e != cudaSuccess)                                                                                 \
+      throw ::pkde::Error{PKDE_ECUDA, std::string("kernel launch at " __FILE__ ":" PKDE_STR(__LINE__) ": ") + \
+                                          cudaGetErrorString(_e)};                                         \
+  } while (0)
 
 inline Error invalid(const char *fmt, ...) {
   char buf[512];
@@ -101,6 +110,10 @@ struct pkde_ctx {
   int step_path = 0;  // PKDE_STEPS_AUTO / PKDE_STEPS_PER_STEP_LAUNCH
   // engine schedule per shape (pkde_set_autotune): key -> {slot MB, tiles per item, delay}
   bool autotune = true;
+  // the tuner may also try ring slots that hold half or all of an estimation's bootstrap
+  // pairs when those exceed 64 MB (off for serving lanes, whose memory admission assumes
+  // slots of at most 64 MB or one pair)
+  bool tune_wide = true;
   bool tune_loaded = false;
   std::map<std::string, std::array<int, 3>> tune;
   // page-locked staging buffer for asynchronous uploads (grow-only)

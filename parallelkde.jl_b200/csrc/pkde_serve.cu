@@ -167,6 +167,7 @@ Server *start_server(pkde_ctx *ctx) {
       delete S;
       throw Error{PKDE_ECUDA, "serving: cannot create a lane context or stream"};
     }
+    c->tune_wide = false;  // the lane's memory budget assumes narrow ring slots
     S->lane_ctx.push_back(c);
     S->lane_stream.push_back(s);
   }

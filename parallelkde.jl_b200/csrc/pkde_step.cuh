@@ -149,6 +149,10 @@ bool engine_register_only(const pkde_grid *g);
 // convergence state (the caller initialises it afterwards).
 void autotune_engine(pkde_ctx *ctx, EngineArgs &args, cudaStream_t st);
 void run_engine(pkde_ctx *ctx, const EngineArgs &args, cudaStream_t st);
+// Device bytes of the estimation's ring slots under its schedule parameters.
+size_t engine_ring_bytes(const EngineArgs &args);
+// Ring slots of at most this size are always allowed; wider ones only within a memory budget.
+constexpr int kNarrowSlotMB = 64;
 // Several estimations in one persistent launch (their EngineArgs are independent).
 void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStream_t st);
 

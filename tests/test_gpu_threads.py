@@ -48,6 +48,7 @@ def test_concurrent_contexts_match_alone(pk):
     errors, results = [], {}
 
     def worker(k):
+        j = None
         try:
             for rep in range(4):
                 for i in range(len(cases)):
@@ -55,7 +56,7 @@ def test_concurrent_contexts_match_alone(pk):
                     g, xt = cases[j]
                     results[(k, rep, j)] = _run(pk, ctxs[k], g, xt, 7 + j)
         except Exception as e:  # reported on the main thread
-            errors.append(repr(e))
+            errors.append(f"thread {k}, shape {SHAPES[j]}: {e!r}")
 
     try:
         threads = [threading.Thread(target=worker, args=(k,)) for k in range(2)]
