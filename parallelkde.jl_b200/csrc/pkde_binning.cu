@@ -273,6 +273,39 @@ __global__ void mult_kernel(int64_t n, int64_t nboot, const int32_t *__restrict_
   }
 }
 
+// counts[b][cell] for the bootstrap resamples, summed from the multiplicities in cell
+// order instead of one atomic per draw: the lanes of a warp hold consecutive (resample,
+// position) entries, a segmented shuffle scan sums equal (resample, cell) keys, and the
+// last lane of each run adds the run's sum with one atomic.
+__global__ void resample_count_kernel(const uint32_t *__restrict__ cell_sorted, int64_t n, int64_t nboot, int64_t G,
+                                      const uint32_t *__restrict__ mult, uint32_t *__restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t total = nboot * n;
+  // the loop bound is rounded up to whole warps, so the shuffles always see all 32 lanes
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d - lane < total; d += stride) {
+    const bool act = d < total;
+    const int64_t b = act ? d / n : 0;
+    const int64_t i = act ? d - b * n : 0;
+    uint32_t v = act ? mult[d] : 0u;
+    const uint32_t c0 = act ? cell_sorted[i] : 0u;
+    const unsigned long long key = act ? (((unsigned long long)b << 32) | c0) : ~0ull - (unsigned long long)lane;
+    bool same[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const unsigned long long up = __shfl_up_sync(0xffffffffu, key, 1 << k);
+      same[k] = lane >= (1 << k) && up == key;
+    }
+    const bool last = __shfl_down_sync(0xffffffffu, key, 1) != key || lane == 31;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, v, 1 << k);
+      if (same[k]) v += u;
+    }
+    if (act && last && v) atomicAdd(&counts[b * G + c0], v);
+  }
+}
+
 // The quantised corner terms of DirectSpace.jl:227-237, stored at the sample's position
 // in cell order (quantize_kernel's arithmetic).
 __global__ void quantize_sorted_kernel(GridDev g, const double *__restrict__ rh, int64_t n, double denom, int e_m,
@@ -545,7 +578,7 @@ void dirac_job_bind(DiracJob &j, char *scratch, int *misc) {
   scratch += al(sizeof(uint32_t) * j.n);
   j.rh = (double *)scratch;
   scratch += al(sizeof(double) * N * j.n + sizeof(unsigned long long) * 2 * nc * j.n);
-  j.counts = (uint32_t *)scratch;
+  j.counts = (uint32_t *)scratch;  // draws per lower cell and resample (slot nboot: identity)
   scratch += al(sizeof(uint32_t) * (j.nboot + 1) * G);
   j.pos = (uint32_t *)scratch;
   scratch += al(sizeof(uint32_t) * j.n);
@@ -592,14 +625,11 @@ void dirac_job_phase_a(pkde_ctx *ctx, DiracJob &j, cudaStream_t st) {
   }
   PKDE_CHECK_LAUNCH();
   {
+    // samples per lower cell (the identity slot); the resamples' counts are summed from
+    // their multiplicities once the samples are in cell order
     ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
-    count_kernel<<<grid_blocks(ctx, nslots * n), kThreads, 0, st>>>(j.cell, n, nslots, j.nboot, G, j.d_idx, j.seed,
-                                                                    j.counts, misc);
-  }
-  PKDE_CHECK_LAUNCH();
-  {
-    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
-    max_kernel<<<grid_blocks(ctx, nslots * G), kThreads, 0, st>>>(j.counts, nslots * G, maxc);
+    count_kernel<<<grid_blocks(ctx, n), kThreads, 0, st>>>(j.cell, n, 1, 0, G, nullptr, 0, j.counts + j.nboot * G,
+                                                          misc);
   }
   PKDE_CHECK_LAUNCH();
   // samples in lower-cell order (counting sort from the identity counts), then each
@@ -635,6 +665,17 @@ void dirac_job_phase_a(pkde_ctx *ctx, DiracJob &j, cudaStream_t st) {
     }
     PKDE_CHECK_LAUNCH();
   }
+  if (j.nboot > 0) {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    resample_count_kernel<<<grid_blocks(ctx, j.nboot * n), kThreads, 0, st>>>(j.cell_sorted, n, j.nboot, G, j.mult,
+                                                                              j.counts);
+  }
+  PKDE_CHECK_LAUNCH();
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    max_kernel<<<grid_blocks(ctx, nslots * G), kThreads, 0, st>>>(j.counts, nslots * G, maxc);
+  }
+  PKDE_CHECK_LAUNCH();
 }
 
 // Phase B, given misc[0..1] read back: error check, fixed-point scales, quantised
