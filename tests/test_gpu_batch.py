@@ -215,3 +215,37 @@ def test_engine_schedules_keep_results(pk, monkeypatch, dims):
         lib.pkde_destroy(ctx)
     for d, s in outs[1:]:
         assert np.array_equal(d, outs[0][0]) and np.array_equal(s, outs[0][1])
+
+
+def test_wide_ring_slots_keep_results(pk, monkeypatch):
+    """Ring slots above 64 MB, holding all bootstrap pairs of a step in one group (what the
+    autotuner picks for large grids), give the same result as narrow slots of one or a
+    few pairs per group."""
+    import ctypes
+    from pkde_b200 import _lib
+    lib = _lib.load()
+    rng = np.random.default_rng(21)
+    x = rng.standard_normal((2, 20000))
+    dims = (256, 256)
+    grid = pk.find_grid(x, grid_dims=dims)
+    B = 80  # 40 pairs x 2 arrays x 1 MB = 80 MB per group of all pairs
+    p = _lib.make_params(_lib.make_grid_struct(grid.lo, grid.hi, grid.h, grid.dims), B, 12)
+    data = np.ascontiguousarray(x.T)
+    G = int(np.prod(dims))
+    ctx = ctypes.c_void_p()
+    assert lib.pkde_create(ctypes.byref(ctx), 0) == 0
+    outs = []
+    try:
+        assert lib.pkde_set_autotune(ctx, 0) == 0
+        for slot_mb, tpi in ((128, 4), (2, 2), (8, 4), (48, 2)):
+            monkeypatch.setenv("PKDE_ENGINE_SLOT_MB", str(slot_mb))
+            monkeypatch.setenv("PKDE_ENGINE_TPI", str(tpi))
+            d, s = np.empty(G), np.empty(G, dtype=np.int32)
+            rc = lib.pkde_gradepro_estimate(ctx, ctypes.byref(p), _lib.ptr(data), data.shape[0], None, 9, _lib.ptr(d),
+                                            _lib.ptr(s), 0, None)
+            _lib.check(rc, ctx)
+            outs.append((d, s))
+    finally:
+        lib.pkde_destroy(ctx)
+    for d, s in outs[1:]:
+        assert np.array_equal(d, outs[0][0]) and np.array_equal(s, outs[0][1])
