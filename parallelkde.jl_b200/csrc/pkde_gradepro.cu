@@ -15,10 +15,8 @@
 //   state    : f_prev1, f_prev2, minima (FP64), counters_low/over (u16), flags (u8),
 //              density (FP64), selected step (i32), final-step means (FP64).
 #include <algorithm>
-#include <atomic>
 #include <cstring>
 #include <limits>
-#include <thread>
 
 #include "pkde_internal.cuh"
 #include "pkde_step.cuh"
@@ -254,6 +252,13 @@ __global__ void moments_final_kernel(const MomentJob *jobs) {
   }
 }
 
+// The means of the first pass, sum / n with one correctly rounded division per axis (the
+// same value the host's division gives), written where the second pass's jobs read them.
+__global__ void moments_mean_kernel(const MomentJob *jobs, double *means) {
+  const MomentJob J = jobs[blockIdx.x];
+  if ((int)threadIdx.x < J.ndim) means[4 * blockIdx.x + threadIdx.x] = __ddiv_rn(J.out[threadIdx.x], (double)J.n);
+}
+
 int blocks_for(pkde_ctx *ctx, int64_t work) {
   int64_t b = (work + kThreads - 1) / kThreads;
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)ctx->sm_count * 8));
@@ -353,12 +358,14 @@ Ladder make_ladder(const pkde_gradepro_params *p, const double *bw_final, int64_
 }
 
 // Per-axis sums of squared deviations from the mean, sum_i (x_ji - mean_j)^2, of several
-// sample sets at once (FP64, deterministic): two reductions, two read-backs for the whole
-// set.  data[e] is N[e] x n[e]; the result goes to centered[4e .. 4e+N[e]-1].
+// sample sets at once (FP64, deterministic): a reduction for the sums, the means on the
+// device, a reduction for the squared deviations, and one read-back for the whole set.
+// data[e] is N[e] x n[e]; the result goes to centered[4e .. 4e+N[e]-1].
 void sample_centered_sums(pkde_ctx *ctx, int count, const double *const *data, const int64_t *n, const int *N,
                           double *centered, cudaStream_t st) {
   if (count < 1) return;
-  std::vector<MomentJob> jobs(count);
+  // jobs[0..count): the sums; jobs[count..2 count): the squared deviations from the means
+  std::vector<MomentJob> jobs(2 * (size_t)count);
   int maxnb = 1;
   size_t npart = 0;
   for (int e = 0; e < count; ++e) {
@@ -367,7 +374,7 @@ void sample_centered_sums(pkde_ctx *ctx, int count, const double *const *data, c
     npart += 4 * (size_t)jobs[e].nb;
   }
   // device: [jobs][sums count x 4][means count x 4][partials]
-  const size_t jb = (sizeof(MomentJob) * count + 255) & ~size_t(255);
+  const size_t jb = (sizeof(MomentJob) * 2 * count + 255) & ~size_t(255);
   char *m = (char *)ensure(ctx, BUF_MISC, jb + sizeof(double) * (8 * (size_t)count + npart));
   MomentJob *djobs = (MomentJob *)m;
   double *sums = (double *)(m + jb), *means = sums + 4 * count, *partial = means + 4 * count;
@@ -379,30 +386,31 @@ void sample_centered_sums(pkde_ctx *ctx, int count, const double *const *data, c
     partial += 4 * (size_t)jobs[e].nb;
     jobs[e].mean = nullptr;
     jobs[e].out = sums + 4 * e;
+    jobs[count + e] = jobs[e];
+    jobs[count + e].mean = means + 4 * e;
+  }
+  PKDE_CUDA_TRY(cudaMemcpyAsync(djobs, jobs.data(), sizeof(MomentJob) * 2 * count, cudaMemcpyHostToDevice, st));
+  for (int pass = 0; pass < 2; ++pass) {
+    const MomentJob *pj = djobs + (size_t)pass * count;
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+      moments_partial_kernel<<<dim3((unsigned)maxnb, (unsigned)count), kThreads, 0, st>>>(pj);
+    }
+    PKDE_CHECK_LAUNCH();
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+      moments_final_kernel<<<(unsigned)count, 32, 0, st>>>(pj);
+    }
+    PKDE_CHECK_LAUNCH();
+    if (pass == 0) {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+      moments_mean_kernel<<<(unsigned)count, 32, 0, st>>>(pj, means);
+    }
+    if (pass == 0) PKDE_CHECK_LAUNCH();
   }
   std::vector<double> h(4 * (size_t)count);
-  for (int pass = 0; pass < 2; ++pass) {
-    if (pass == 1)
-      for (int e = 0; e < count; ++e) jobs[e].mean = means + 4 * e;
-    PKDE_CUDA_TRY(cudaMemcpyAsync(djobs, jobs.data(), sizeof(MomentJob) * count, cudaMemcpyHostToDevice, st));
-    {
-      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-      moments_partial_kernel<<<dim3((unsigned)maxnb, (unsigned)count), kThreads, 0, st>>>(djobs);
-    }
-    PKDE_CHECK_LAUNCH();
-    {
-      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
-      moments_final_kernel<<<(unsigned)count, 32, 0, st>>>(djobs);
-    }
-    PKDE_CHECK_LAUNCH();
-    PKDE_CUDA_TRY(cudaMemcpyAsync(h.data(), sums, sizeof(double) * 4 * count, cudaMemcpyDeviceToHost, st));
-    PKDE_CUDA_TRY(cudaStreamSynchronize(st));
-    if (pass == 0) {
-      for (int e = 0; e < count; ++e)
-        for (int j = 0; j < N[e]; ++j) h[4 * e + j] /= (double)n[e];
-      PKDE_CUDA_TRY(cudaMemcpyAsync(means, h.data(), sizeof(double) * 4 * count, cudaMemcpyHostToDevice, st));
-    }
-  }
+  PKDE_CUDA_TRY(cudaMemcpyAsync(h.data(), sums, sizeof(double) * 4 * count, cudaMemcpyDeviceToHost, st));
+  PKDE_CUDA_TRY(cudaStreamSynchronize(st));
   std::memcpy(centered, h.data(), sizeof(double) * 4 * count);
 }
 
@@ -455,25 +463,34 @@ static void factor_tables(const pkde_grid *g, const Ladder &L, std::vector<doubl
 }
 
 // The same tables written straight into fz/fw (S x tot each), steps [s0, s1).
-static void fill_factor_tables(const pkde_grid *g, const Ladder &L, const std::vector<int64_t> &axis_off, double *fz,
-                               double *fw, int64_t s0, int64_t s1) {
-  const int N = g->ndim;
-  const int64_t tot = axis_off[N];
-  const double two_pi = 6.283185307179586;
-  for (int64_t s = s0; s < s1; ++s) {
-    for (int j = 0; j < N; ++j) {
-      const int64_t n = g->dims[j];
-      const double mult = two_pi * ((1.0 / g->h[j]) / (double)n);
-      const double t = L.times[s * N + j];
-      const int64_t nneg = (n - 1) / 2 + 1;
-      for (int64_t m = 0; m < n; ++m) {
-        const double mm = (double)(m < nneg ? m : m - n);
-        const double kt = (mm * mult) * t;
-        const double pv = std::exp(-0.5 * (kt * kt));
-        fz[s * tot + axis_off[j] + m] = pv;
-        fw[s * tot + axis_off[j] + m] = std::sqrt(pv);
-      }
-    }
+// Propagation factor tables of one estimation, computed on the device: for step s and
+// grid axis j, fz = exp(-(k t)^2 / 2) and fw = sqrt(fz) over the axis's frequencies k =
+// 2 pi fftfreq(n, h) (FourierSpace.jl:228-234 per axis; the full propagator is their
+// product over the axes).  Same operation order as the reference's per-axis terms; exp is
+// CUDA's, so a factor can differ from a CPU exp in the last bit.
+struct TableJob {
+  double *fz;            // [S][tot] fz, then [S][tot] fw
+  const double *times;   // [S][N]
+  int64_t S, tot;
+  int N;
+  int64_t aoff[5];
+  int64_t dims[4];
+  double mult[4];        // 2 pi ((1 / h) / n) per axis
+};
+
+__global__ void factor_table_kernel(const TableJob *jobs) {
+  const TableJob J = jobs[blockIdx.y];
+  const int64_t total = J.S * J.tot;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = i / J.tot, r = i - s * J.tot;
+    int j = 0;
+    while (j + 1 < J.N && r >= J.aoff[j + 1]) ++j;
+    const int64_t n = J.dims[j], m = r - J.aoff[j], nneg = (n - 1) / 2 + 1;
+    const double mm = (double)(m < nneg ? m : m - n);
+    const double kt = __dmul_rn(__dmul_rn(mm, J.mult[j]), J.times[s * J.N + j]);
+    const double pv = exp(__dmul_rn(-0.5, __dmul_rn(kt, kt)));
+    J.fz[i] = pv;
+    J.fz[total + i] = sqrt(pv);
   }
 }
 
@@ -727,6 +744,11 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
   // 1-D per-step arrays, binning scratch]
   const size_t off_tables = arena;
   arena += tables_bytes;
+  size_t times_doubles = 0;
+  for (int e = 0; e < count; ++e) times_doubles += (size_t)plans[e].L.S * plans[e].N;
+  const size_t tjob_bytes = al256(sizeof(TableJob) * count) + al256(sizeof(double) * times_doubles);
+  const size_t off_tjobs = arena;
+  arena += tjob_bytes;
   for (int e = 0; e < count; ++e) {
     Plan &P = plans[e];
     off[e] = arena;
@@ -777,33 +799,39 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
   }
   // ---- binning: phase A for all (queued first, so that the host work below overlaps it)
   for (int e = 0; e < count; ++e) dirac_job_phase_a(ctx, plans[e].job, st);
-  // ---- propagation factor tables: host threads into page-locked memory, one async upload
+  // ---- propagation factor tables, on the device: the ladders' times and the job
+  // descriptors go up in one copy from page-locked memory, one kernel fills every table
   if (tables_bytes) {
-    char *hp = (char *)pinned_staging(ctx, tables_bytes);
-    struct Chunk {
-      int e;
-      int64_t s0, s1;
-    };
-    std::vector<Chunk> chunks;
+    char *hp = (char *)pinned_staging(ctx, tjob_bytes);
+    TableJob *hj = (TableJob *)hp;
+    double *ht = (double *)(hp + al256(sizeof(TableJob) * count));
+    const double *dt = (const double *)(base + off_tjobs + al256(sizeof(TableJob) * count));
+    const double two_pi = 6.283185307179586;
+    int64_t tpos = 0, maxtotal = 1;
     for (int e = 0; e < count; ++e) {
-      const int64_t S = plans[e].L.S, per = std::max<int64_t>(1, (int64_t)(1 << 16) / std::max<int64_t>(1, plans[e].tot));
-      for (int64_t s0 = 0; s0 < S; s0 += per) chunks.push_back({e, s0, std::min(S, s0 + per)});
-    }
-    const int nth = (int)std::min<size_t>(chunks.size(), std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
-    std::atomic<size_t> next{0};
-    auto work = [&] {
-      for (size_t k; (k = next.fetch_add(1)) < chunks.size();) {
-        const Chunk &c = chunks[k];
-        const Plan &P = plans[c.e];
-        double *fz = (double *)(hp + toffs[c.e]);
-        fill_factor_tables(P.g, P.L, P.aoff, fz, fz + P.L.S * P.tot, c.s0, c.s1);
+      const Plan &P = plans[e];
+      TableJob &J = hj[e];
+      J.fz = P.tables;
+      J.S = P.L.S;
+      J.tot = P.tot;
+      J.N = P.N;
+      for (int q = 0; q <= P.N; ++q) J.aoff[q] = P.aoff[q];
+      for (int q = 0; q < P.N; ++q) {
+        J.dims[q] = P.g->dims[q];
+        J.mult[q] = two_pi * ((1.0 / P.g->h[q]) / (double)P.g->dims[q]);
       }
-    };
-    std::vector<std::thread> pool;
-    for (int i = 1; i < nth; ++i) pool.emplace_back(work);
-    work();
-    for (auto &t : pool) t.join();
-    PKDE_CUDA_TRY(cudaMemcpyAsync(base + off_tables, hp, tables_bytes, cudaMemcpyHostToDevice, st));
+      std::memcpy(ht + tpos, P.L.times.data(), sizeof(double) * P.L.S * P.N);
+      J.times = dt + tpos;
+      tpos += P.L.S * P.N;
+      maxtotal = std::max<int64_t>(maxtotal, P.L.S * P.tot);
+    }
+    PKDE_CUDA_TRY(cudaMemcpyAsync(base + off_tjobs, hp, tjob_bytes, cudaMemcpyHostToDevice, st));
+    {
+      ::pkde::Trace _tr(ctx, PKDE_PHASE_OTHER, st);
+      const unsigned bx = (unsigned)std::min<int64_t>((maxtotal + kThreads - 1) / kThreads, (int64_t)ctx->sm_count * 4);
+      factor_table_kernel<<<dim3(bx, (unsigned)count), kThreads, 0, st>>>((const TableJob *)(base + off_tjobs));
+    }
+    PKDE_CHECK_LAUNCH();
   }
   std::vector<int> hmisc(64 * (size_t)count);
   PKDE_CUDA_TRY(cudaMemcpyAsync(hmisc.data(), base, 256 * (size_t)count, cudaMemcpyDeviceToHost, st));
