@@ -71,6 +71,7 @@ int pkde_destroy(pkde_ctx *ctx) {
   cudaDeviceSynchronize();
   for (auto &b : ctx->buf) b.release();
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->engine_flags) cudaFreeHost(ctx->engine_flags);
   delete ctx;
   return PKDE_OK;
 }

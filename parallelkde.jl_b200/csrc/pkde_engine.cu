@@ -1227,10 +1227,22 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
     kern<<<(unsigned)grid, kEngineThreads, smem, st>>>(R, (int)max_tile, (int)state_elems);
   }
   PKDE_CHECK_LAUNCH();
-  int err = 0;
-  PKDE_CUDA_TRY(cudaMemcpyAsync(&err, R.error, sizeof(int), cudaMemcpyDeviceToHost, st));
-  PKDE_CUDA_TRY(cudaStreamSynchronize(st));
-  if (err) throw Error{PKDE_ECUDA, "step engine: a dependency wait timed out (run aborted)"};
+  // the launch's error flag comes back with the call's own synchronisation
+  constexpr int kEngineFlags = 64;
+  if (!ctx->engine_flags) PKDE_CUDA_TRY(cudaMallocHost(&ctx->engine_flags, sizeof(int) * kEngineFlags));
+  if (ctx->engine_flags_used == kEngineFlags) {  // every slot in use: check them first
+    PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+    check_engine_flags(ctx);
+  }
+  int *flag = ctx->engine_flags + ctx->engine_flags_used++;
+  PKDE_CUDA_TRY(cudaMemcpyAsync(flag, R.error, sizeof(int), cudaMemcpyDeviceToHost, st));
+}
+
+void check_engine_flags(pkde_ctx *ctx) {
+  bool bad = false;
+  for (int i = 0; i < ctx->engine_flags_used; ++i) bad |= ctx->engine_flags[i] != 0;
+  ctx->engine_flags_used = 0;
+  if (bad) throw Error{PKDE_ECUDA, "step engine: a dependency wait timed out (run aborted)"};
 }
 
 void run_engine(pkde_ctx *ctx, const EngineArgs &A, cudaStream_t st) { run_engine_batch(ctx, &A, 1, st); }
@@ -1323,6 +1335,7 @@ void autotune_engine(pkde_ctx *ctx, EngineArgs &A, cudaStream_t st) {
       run_engine_batch(ctx, &T, 1, st);
       PKDE_CUDA_TRY(cudaEventRecord(e1, st));
       PKDE_CUDA_TRY(cudaEventSynchronize(e1));
+      check_engine_flags(ctx);
       float ms = 0.f;
       PKDE_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
       return ms;

@@ -1097,6 +1097,10 @@ int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradep
       E.d_density = dens;
       E.d_selected = sel;
     }
+    if (ctx->engine_flags_used) {  // flags left by a call that failed before its check
+      PKDE_CUDA_TRY(cudaDeviceSynchronize());
+      ctx->engine_flags_used = 0;
+    }
     run_many(ctx, ests.data(), count, st);
     if (!dout) {
       for (int e = 0; e < count; ++e) {
@@ -1107,6 +1111,7 @@ int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradep
     }
     PKDE_CUDA_TRY(cudaStreamSynchronize(st));
     collect_trace(ctx);
+    check_engine_flags(ctx);
   });
 }
 

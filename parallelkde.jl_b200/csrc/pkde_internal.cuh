@@ -116,6 +116,10 @@ struct pkde_ctx {
   bool tune_wide = true;
   bool tune_loaded = false;
   std::map<std::string, std::array<int, 3>> tune;
+  // step-engine error flags, copied back without a synchronisation of their own and
+  // checked when the call synchronises (check_engine_flags); page-locked
+  int *engine_flags = nullptr;
+  int engine_flags_used = 0;
   // page-locked staging buffer for asynchronous uploads (grow-only)
   void *pinned = nullptr;
   size_t pinned_bytes = 0;

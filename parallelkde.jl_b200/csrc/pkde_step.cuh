@@ -149,6 +149,9 @@ bool engine_register_only(const pkde_grid *g);
 // convergence state (the caller initialises it afterwards).
 void autotune_engine(pkde_ctx *ctx, EngineArgs &args, cudaStream_t st);
 void run_engine(pkde_ctx *ctx, const EngineArgs &args, cudaStream_t st);
+// The error flags of the engine launches queued since the last check: call after the stream
+// has synchronised; throws if a launch gave up on a dependency wait.
+void check_engine_flags(pkde_ctx *ctx);
 // Device bytes of the estimation's ring slots under its schedule parameters.
 size_t engine_ring_bytes(const EngineArgs &args);
 // Ring slots of at most this size are always allowed; wider ones only within a memory budget.
