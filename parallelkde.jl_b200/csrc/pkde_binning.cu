@@ -308,11 +308,12 @@ __global__ void resample_count_kernel(const uint32_t *__restrict__ cell_sorted, 
 
 // The quantised corner terms of DirectSpace.jl:227-237, stored at the sample's position
 // in cell order (quantize_kernel's arithmetic).
-__global__ void quantize_sorted_kernel(GridDev g, const double *__restrict__ rh, int64_t n, double denom, int e_m,
-                                       int e_v, const uint32_t *__restrict__ pos, unsigned long long *__restrict__ qm,
-                                       unsigned long long *__restrict__ qv) {
+__global__ void quantize_sorted_kernel(GridDev g, const double *__restrict__ rh, int64_t n, double denom,
+                                       const int *__restrict__ esc, const uint32_t *__restrict__ pos,
+                                       unsigned long long *__restrict__ qm, unsigned long long *__restrict__ qv) {
   int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= n) return;
+  const int e_m = esc[0], e_v = esc[1];
   const int N = g.ndim;
   const int64_t ps = pos[s];
   double r_h[4], r_l[4];
@@ -407,6 +408,34 @@ __global__ void dequant_kernel(unsigned long long *v, int64_t m, double scale) {
 
 __global__ void dequant_paired_kernel(unsigned long long *v, int64_t G, int64_t npairs, double sm, double sv) {
   // arrays: [z0, w0, z1, w1, ..., zF]; w arrays use sv
+  const int64_t total = (2 * npairs + 1) * G * 2;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t arr = i / (2 * G);
+    double sc = (arr < 2 * npairs && (arr & 1)) ? sv : sm;
+    unsigned long long x = v[i];
+    reinterpret_cast<double *>(v)[i] = (double)x * sc;
+  }
+}
+
+// The fixed-point exponents of a binning job from its largest count (misc[1]), on the
+// device so that phase B needs no read-back: a cell sums at most 2^N * cmax terms, each
+// <= tmax (means) or tmax^2 (second moments); e = 62 - the binary exponent of that bound.
+// esc[0] = e_m, esc[1] = e_v.  The same operations, in the same order, as on the host.
+__global__ void scale_exponents_kernel(const int *misc, double nc, double tmax, int *esc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double cmax = (double)(uint32_t)misc[1];
+  const double bm = __dmul_rn(__dmul_rn(nc, cmax > 1.0 ? cmax : 1.0), tmax);
+  const double bv = __dmul_rn(bm, tmax);
+  int ex_m, ex_v;
+  frexp(bm, &ex_m);
+  frexp(bv, &ex_v);
+  esc[0] = 62 - ex_m;
+  esc[1] = 62 - ex_v;
+}
+
+// dequant_paired_kernel with the scales 2^-e_m, 2^-e_v from device memory
+__global__ void dequant_paired_esc_kernel(unsigned long long *v, int64_t G, int64_t npairs, const int *esc) {
+  const double sm = ldexp(1.0, -esc[0]), sv = ldexp(1.0, -esc[1]);
   const int64_t total = (2 * npairs + 1) * G * 2;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     int64_t arr = i / (2 * G);
@@ -680,13 +709,16 @@ void dirac_job_phase_a(pkde_ctx *ctx, DiracJob &j, cudaStream_t st) {
 
 // Phase B, given misc[0..1] read back: error check, fixed-point scales, quantised
 // corner terms, scatter into the paired spectra slots, conversion to FP64.
-void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_t st) {
-  const pkde_grid *g = j.g;
+void binning_flags_check(const int *hmisc) {
   if (hmisc[0] & 1) throw invalid("Data points lie beyond grid. Remove them or increase grid boundaries.");
   if (hmisc[0] & 2)
     throw invalid("Data points lie within one rounding of the upper grid bound. Remove them or increase grid boundaries.");
   if (hmisc[0] & 4) throw invalid("Bootstrap indices must lie in 1:n_samples.");
-  const double cmax = (double)(uint32_t)hmisc[1];
+}
+
+void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_t st) {
+  const pkde_grid *g = j.g;
+  if (hmisc) binning_flags_check(hmisc);
   GridDev gd = to_dev(g);
   const int64_t G = grid_size(g);
   const int N = g->ndim;
@@ -697,25 +729,23 @@ void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_
   unsigned long long *qm = reinterpret_cast<unsigned long long *>(j.rh + N * n);
   unsigned long long *qv = qm + (int64_t)nc * n;
   const int64_t *corner_off = reinterpret_cast<const int64_t *>(j.misc + 8);
+  int *esc = j.misc + 48;
   // term <= prod(h) / (n prod(h)^2); a cell sums at most 2^N * cmax terms.
   double sp = g->h[0];
   for (int q = 1; q < N; ++q) sp = sp * g->h[q];
   const double denom = (double)n * (sp * sp);
   const double tmax = (1.0 / ((double)n * sp)) * (1.0 + 1e-12);
-  const double bound_m = (double)nc * std::max(cmax, 1.0) * tmax;
-  const double bound_v = (double)nc * std::max(cmax, 1.0) * tmax * tmax;
-  int ex_m, ex_v;
-  std::frexp(bound_m, &ex_m);  // bound_m < 2^ex_m
-  std::frexp(bound_v, &ex_v);
-  const int e_m = 62 - ex_m;
-  const int e_v = 62 - ex_v;
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
-    quantize_sorted_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(gd, j.rh, n, denom, e_m,
-                                                                                            e_v, j.pos, qm, qv);
+    scale_exponents_kernel<<<1, 32, 0, st>>>(j.misc, (double)nc, tmax, esc);
   }
   PKDE_CHECK_LAUNCH();
-  const double sm = std::ldexp(1.0, -e_m), sv = std::ldexp(1.0, -e_v);
+  {
+    ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
+    quantize_sorted_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(gd, j.rh, n, denom, esc,
+                                                                                            j.pos, qm, qv);
+  }
+  PKDE_CHECK_LAUNCH();
   const int64_t npairs = (nboot + 1) / 2;
   unsigned long long *acc = reinterpret_cast<unsigned long long *>(j.paired_out);
   PKDE_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double2) * (2 * npairs + 1) * G, st));
@@ -736,7 +766,7 @@ void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_
   PKDE_CHECK_LAUNCH();
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
-    dequant_paired_kernel<<<grid_blocks(ctx, (2 * npairs + 1) * G * 2), kThreads, 0, st>>>(acc, G, npairs, sm, sv);
+    dequant_paired_esc_kernel<<<grid_blocks(ctx, (2 * npairs + 1) * G * 2), kThreads, 0, st>>>(acc, G, npairs, esc);
   }
   PKDE_CHECK_LAUNCH();
 }

@@ -504,6 +504,21 @@ static void axis_offsets(const pkde_grid *g, std::vector<int64_t> &axis_off) {
   axis_off[g->ndim] = tot;
 }
 
+// The binning error flags of the call's estimations (after its final synchronisation).
+static void check_binning_flags(pkde_ctx *ctx) {
+  const int count = ctx->bin_flags_count;
+  ctx->bin_flags_count = 0;
+  for (int e = 0; e < count; ++e) {
+    try {
+      binning_flags_check(ctx->bin_flags + 64 * (size_t)e);
+    } catch (Error &err) {
+      if (count > 1) err.msg = "estimation " + std::to_string(e) + ": " + err.msg;
+      ctx->engine_flags_used = 0;  // the call fails on its data; the engine's flags are moot
+      throw;
+    }
+  }
+}
+
 // Page-locked staging buffer of the context (grow-only), for asynchronous uploads.
 static void *pinned_staging(pkde_ctx *ctx, size_t bytes) {
   if (bytes > ctx->pinned_bytes) {
@@ -801,8 +816,8 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
   for (int e = 0; e < count; ++e) dirac_job_phase_a(ctx, plans[e].job, st);
   // ---- propagation factor tables, on the device: the ladders' times and the job
   // descriptors go up in one copy from page-locked memory, one kernel fills every table
+  char *hp = (char *)pinned_staging(ctx, al256(tjob_bytes) + 256 * (size_t)count);
   if (tables_bytes) {
-    char *hp = (char *)pinned_staging(ctx, tjob_bytes);
     TableJob *hj = (TableJob *)hp;
     double *ht = (double *)(hp + al256(sizeof(TableJob) * count));
     const double *dt = (const double *)(base + off_tjobs + al256(sizeof(TableJob) * count));
@@ -833,17 +848,13 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
     }
     PKDE_CHECK_LAUNCH();
   }
-  std::vector<int> hmisc(64 * (size_t)count);
-  PKDE_CUDA_TRY(cudaMemcpyAsync(hmisc.data(), base, 256 * (size_t)count, cudaMemcpyDeviceToHost, st));
-  PKDE_CUDA_TRY(cudaStreamSynchronize(st));
-  for (int e = 0; e < count; ++e) {
-    try {
-      dirac_job_phase_b(ctx, plans[e].job, &hmisc[64 * (size_t)e], st);
-    } catch (Error &err) {
-      if (count > 1) err.msg = "estimation " + std::to_string(e) + ": " + err.msg;
-      throw;
-    }
-  }
+  // the binning error flags come back with the call's final synchronisation (invalid data
+  // is reported then; what runs on it meanwhile stays in bounds: such samples bin to cell 0)
+  int *hflags = (int *)(hp + al256(tjob_bytes));
+  PKDE_CUDA_TRY(cudaMemcpyAsync(hflags, base, 256 * (size_t)count, cudaMemcpyDeviceToHost, st));
+  ctx->bin_flags = hflags;
+  ctx->bin_flags_count = count;
+  for (int e = 0; e < count; ++e) dirac_job_phase_b(ctx, plans[e].job, nullptr, st);
   // ---- forward FFT of every array
   for (int e = 0; e < count; ++e)
     fft_nd(ctx, plans[e].N, plans[e].g->dims, plans[e].spectra, 2 * plans[e].npairs + 1, -1, st,
@@ -1111,6 +1122,7 @@ int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradep
     }
     PKDE_CUDA_TRY(cudaStreamSynchronize(st));
     collect_trace(ctx);
+    check_binning_flags(ctx);
     check_engine_flags(ctx);
   });
 }

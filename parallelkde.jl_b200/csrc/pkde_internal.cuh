@@ -120,6 +120,10 @@ struct pkde_ctx {
   // checked when the call synchronises (check_engine_flags); page-locked
   int *engine_flags = nullptr;
   int engine_flags_used = 0;
+  // binning error flags of the estimations of the call in flight (64 ints each, in the
+  // page-locked staging buffer), checked after the call's final synchronisation
+  const int *bin_flags = nullptr;
+  int bin_flags_count = 0;
   // page-locked staging buffer for asynchronous uploads (grow-only)
   void *pinned = nullptr;
   size_t pinned_bytes = 0;
@@ -557,7 +561,10 @@ struct DiracJob {
 size_t dirac_job_scratch(const pkde_grid *g, int64_t n, int64_t nboot);
 void dirac_job_bind(DiracJob &j, char *scratch, int *misc);
 void dirac_job_phase_a(pkde_ctx *ctx, DiracJob &j, cudaStream_t st);
+// hmisc: misc[0..1] read back (checked here), or nullptr: the caller checks the error flags
+// (binning_flags_check) after the call has synchronised; the scales come from the device.
 void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_t st);
+void binning_flags_check(const int *hmisc);
 
 void fft_nd(pkde_ctx *ctx, int ndim, const int64_t *dims, double2 *data, int64_t batch, int dir,
             cudaStream_t st, int phase);
