@@ -1108,9 +1108,10 @@ int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradep
       E.d_density = dens;
       E.d_selected = sel;
     }
-    if (ctx->engine_flags_used) {  // flags left by a call that failed before its check
-      PKDE_CUDA_TRY(cudaDeviceSynchronize());
+    if (ctx->engine_flags_used || ctx->bin_flags_count) {  // flags left by a call that failed before its
+      PKDE_CUDA_TRY(cudaDeviceSynchronize());              // check: their copies land before reuse
       ctx->engine_flags_used = 0;
+      ctx->bin_flags_count = 0;
     }
     run_many(ctx, ests.data(), count, st);
     if (!dout) {
