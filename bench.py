@@ -69,13 +69,14 @@ class Clocks:
     """nvidia-smi sampling during the timed region."""
 
     def __init__(self, index):
+        import tempfile
         self.index = index
         self.proc = None
-        self.path = os.path.join(REPO, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="pkde_clocks_", suffix=".csv")
+        os.close(fd)
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -107,6 +108,10 @@ class Clocks:
             for nm, v in zip(names, f[3:7]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
@@ -127,46 +132,129 @@ def dist_setup(args):
 
 
 # ----------------------------------------------------------------------- reference arm
-def cpu_reference(x, gspec, kw, budget_s=20.0, log=None):
-    """The oracle port (FP64, scipy.fft threads + OpenMP binning) on a bounded sample:
-    full binning and forward transforms, then bandwidth steps until ~budget_s."""
-    import math
-    import scipy.fft as sfft
-    from oracle import gradepro as og
-    from oracle.rng import bootstrap_indices
+class ReferenceSampler:
+    """The reference's CPU path for this workload (the FP64 oracle port: OpenMP binning,
+    scipy.fft, NumPy; ParallelKDE.jl itself needs Julia, which is absent) on bounded
+    samples.  setup() does the once-per-estimation work (binning of every resample and
+    of the full sample, forward FFTs, ladder); sample(k) runs k whole bandwidth steps of
+    the reference's loop body (GradeProEstimator.jl:992-1043: propagate, inverse FFTs of
+    all resamples, scaled VMR, means, convergence update), continuing along the ladder.
+    The unit is grid-point.bandwidth-steps, so a sample's throughput needs no
+    extrapolation."""
+
+    def __init__(self, x, gspec, kw, threads):
+        self.x, self.gspec, self.kw, self.threads = x, gspec, kw, threads
+
+    def setup(self):
+        from oracle import gradepro as og
+        from oracle.rng import bootstrap_indices
+        self.og = og
+        x, kw, cores = self.x, self.kw, self.threads
+        self.grid = og.find_grid(x, grid_dims=self.gspec["dims"], grid_padding=self.gspec.get("grid_padding"))
+        n = x.shape[1]
+        self.n = n
+        idx = bootstrap_indices(0, n, kw["n_bootstraps"])
+        t0 = time.perf_counter()
+        Mb, Vb = og.dirac(x, self.grid, idx, nthreads=cores)
+        Mf, _ = og.dirac(x, self.grid, np.arange(1, n + 1, dtype=np.int32)[None], include_var=False, nthreads=cores)
+        self.Mh = og.fourier_statistics(Mb.astype(complex), cores)
+        self.Vh = og.fourier_statistics(Vb.astype(complex), cores)
+        self.Fh = og.fourier_statistics(Mf.astype(complex), cores)[0]
+        self.times, sl, so, eps = og.ladder(x, self.grid, kw["n_steps"])
+        self.tinit = og.initial_bandwidth(self.grid)
+        self.state = og.DensityState(eps, sl, so, self.grid.shape_c)
+        self.density = np.full(self.grid.shape_c, np.nan)
+        self.s = 0
+        self.setup_s = time.perf_counter() - t0
+        return self.setup_s
+
+    def sample(self, k=1):
+        og, cores, st = self.og, self.threads, self.state
+        t0sq = self.tinit ** 2
+        with np.errstate(all="ignore"):
+            for _ in range(k):
+                s = self.s % len(self.times)
+                t = self.times[s]
+                Mt, Vt = og.propagate_statistics(self.Mh, self.Vh, self.grid, t, self.tinit)
+                f = og.scaled_vmr(og.ifourier_statistics(Mt, True, cores), og.ifourier_statistics(Vt, True, cores), t,
+                                  self.tinit, self.n)
+                means = og.full_means(og.ifourier_statistics(og.propagate_means(self.Fh, self.grid, t), False, cores))
+                dlogt = og.calculate_dlogt(t0sq, t) if s == 0 else og.calculate_dlogt(t0sq, t, self.times[s - 1])
+                og.identify_convergence(self.density, means, f, st.f_prev1, st.f_prev2, dlogt, st.eps, st.steps_low,
+                                        st.steps_over, st.minima, st.counters_low, st.counters_over, st.low_flags)
+                st.f_prev2, st.f_prev1 = st.f_prev1, f
+                self.s += 1
+        return self.grid.size * k
+
+
+def cpu_baseline(x, gspec, kw, budget_s=15.0, serial=True):
+    """cpu_baseline of our arm's line: the oracle port threaded over every host core on
+    bandwidth steps of the workload until ~budget_s, and (serial=True) one bandwidth
+    step on one core (the reference's default method is :serial, Devices.jl:79-83)."""
     cores = os.cpu_count() or 1
-    grid = og.find_grid(x, grid_dims=gspec["dims"], grid_padding=gspec.get("grid_padding"))
-    n = x.shape[1]
-    B = kw["n_bootstraps"]
-    idx = bootstrap_indices(1, n, B)
-    t0 = time.perf_counter()
-    Mb, Vb = og.dirac(x, grid, idx, nthreads=cores)
-    Mf, _ = og.dirac(x, grid, np.arange(1, n + 1, dtype=np.int32)[None], include_var=False, nthreads=cores)
-    Mh = og.fourier_statistics(Mb.astype(complex), cores)
-    Vh = og.fourier_statistics(Vb.astype(complex), cores)
-    Fh = og.fourier_statistics(Mf.astype(complex), cores)[0]
-    t_setup = time.perf_counter() - t0
-    times, sl, so, eps = og.ladder(x, grid, kw["n_steps"])
-    S = len(times)
-    tinit = og.initial_bandwidth(grid)
-    done = 0
-    t1 = time.perf_counter()
-    with np.errstate(all="ignore"):
-        while done < S and (time.perf_counter() - t1) < budget_s:
-            t = times[done]
-            Mt, Vt = og.propagate_statistics(Mh, Vh, grid, t, tinit)
-            og.scaled_vmr(og.ifourier_statistics(Mt, True, cores), og.ifourier_statistics(Vt, True, cores), t, tinit, n)
-            og.full_means(og.ifourier_statistics(og.propagate_means(Fh, grid, t), False, cores))
-            done += 1
-    t_steps = time.perf_counter() - t1
-    G = grid.size
-    per_step = t_steps / done
-    t_full = t_setup + per_step * S
-    value = G * S / t_full
-    sample = (f"oracle FP64 port, {cores} threads: binning + forward FFTs of all {B} resamples ({t_setup:.1f} s) "
-              f"and {done} of {S} bandwidth steps ({t_steps:.1f} s); full-estimation time extrapolated "
-              f"as setup + {S} x per-step = {t_full:.1f} s")
-    return dict(value=value, unit=UNIT, cores=cores, kind="port", sample=sample, est_per_s=1.0 / t_full)
+    ref = ReferenceSampler(x, gspec, kw, cores)
+    setup_s = ref.setup()
+    S = len(ref.times)
+    units, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < budget_s and ref.s < S:
+        units += ref.sample(1)
+    dt = time.perf_counter() - t0
+    out = dict(value=units / dt, unit=UNIT, cores=cores, kind="port",
+               sample=(f"oracle FP64 port on {cores} threads: {units // ref.grid.size} bandwidth steps of the workload "
+                       f"(all {kw['n_bootstraps']} resamples, convergence update included) in {dt:.1f} s; "
+                       f"binning + forward FFTs once per estimation took {setup_s:.1f} s (not in the value)"))
+    if serial:
+        one = ReferenceSampler(x, gspec, kw, 1)
+        one.setup()
+        t1 = time.perf_counter()
+        u = one.sample(1)
+        ts = time.perf_counter() - t1
+        out["serial"] = dict(value=u / ts, unit=UNIT, cores=1, kind="port",
+                             sample=f"one bandwidth step on 1 thread ({ts:.1f} s)")
+    return out
+
+
+def run_reference(args, x, gspec, kw, config, rank, dist):
+    """--impl reference: rank 0 times the reference's CPU path; each step is one bounded
+    sample (--ref-bandwidth-steps whole bandwidth steps of the workload's estimation,
+    every host thread), so steps, ms_per_step and value are all measured."""
+    if rank == 0:
+        cores = os.cpu_count() or 1
+        ref = ReferenceSampler(x, gspec, kw, cores)
+        setup_s = ref.setup()
+        k = max(1, args.ref_bandwidth_steps)
+        for _ in range(args.warmup):
+            ref.sample(k)
+        units, t0 = 0, time.perf_counter()
+        for _ in range(args.steps):
+            units += ref.sample(k)
+        dt = time.perf_counter() - t0
+        value = units / dt
+        serial = None
+        if not args.no_serial:
+            one = ReferenceSampler(x, gspec, kw, 1)
+            one.setup()
+            t1 = time.perf_counter()
+            u = one.sample(1)
+            serial = dict(value=u / (time.perf_counter() - t1), unit=UNIT, cores=1, kind="port",
+                          sample="one bandwidth step on 1 thread (the reference's default :serial method)")
+        S = len(ref.times)
+        sample = (f"oracle FP64 port (the reference's CPU path restated; Julia is absent) on {cores} threads; each step "
+                  f"= {k} whole bandwidth step(s) of the workload's estimation: propagate, inverse FFTs of all "
+                  f"{kw['n_bootstraps']} resamples, scaled VMR, means, convergence update; binning + forward FFTs "
+                  f"once ({setup_s:.1f} s per estimation, outside the timed steps)")
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": config,
+                "estimations_per_s_derived": 1.0 / (setup_s + S * (dt / (args.steps * k))),
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if serial:
+            line["cpu_baseline"]["serial"] = serial
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------------------- our arm
@@ -181,13 +269,27 @@ def main():
     ap.add_argument("--requests", type=int, default=64, help="requests (--workload served)")
     ap.add_argument("--lanes", type=int, default=2, help="serving lanes (--workload served)")
     ap.add_argument("--batch", type=int, default=256, help="estimations per batch (--workload batched)")
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-mix record that the default (c2) run appends")
+    ap.add_argument("--batched-steps", type=int, default=2, help="timed batch calls of the batched-mix record")
+    ap.add_argument("--ref-bandwidth-steps", type=int, default=1,
+                    help="bandwidth steps per timed step of --impl reference")
+    ap.add_argument("--no-serial", action="store_true", help="--impl reference: skip the 1-thread sample")
     ap.add_argument("--bandwidth-steps", type=int, default=None,
                     help="override the workload's bandwidth steps (small profiling runs only)")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
+    if args.workload in ("batched", "batched-small", "served") and args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the single-estimation "
+                              "workloads c1/c2/c3 (the reference estimates one sample set per call)"}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.workload in ("batched", "batched-small"):
         return run_batched(args, world, rank, local, dist)
     if args.workload == "served":
@@ -198,20 +300,15 @@ def main():
     wl_name = {"c1": "1-D N(0,1) n=1e4, 1024 pts, B=100, 251 bandwidths",
                "c2": "2-D 3-GMM n=1e6, 512x512, B=64, 201 bandwidths",
                "c3": "3-D banana+t3 n=4e6, 128^3, B=32, 151 bandwidths"}[args.workload]
+    # the workload only (identical in both arms); measured figures sit outside `config`
+    S_cfg = (kw["n_steps"] or 250) + 1
+    config = {"workload": wl_name, "grid_points": int(np.prod(gspec["dims"])), "bandwidths": S_cfg,
+              "bootstraps": kw["n_bootstraps"], "samples": int(x.shape[1]),
+              "l2": "inputs (spectra 16(B+1)G bytes) larger than the 126 MB L2",
+              "parallelism": f"independent estimations per rank x{world}"}
 
     if args.impl == "reference":
-        if rank == 0:
-            ref = cpu_reference(x, gspec, kw, budget_s=args.cpu_budget)
-            line = {"impl": "reference", "metric": METRIC, "value": ref["value"], "unit": UNIT, "n_gpus": args.gpus,
-                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / ref["est_per_s"],
-                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                    "data": "synthetic", "config": {"workload": wl_name, "estimations_per_s": ref["est_per_s"]},
-                    "cpu_baseline": {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")},
-                    "e2e": {"value": ref["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-            print(json.dumps(line), flush=True)
-        if dist:
-            dist.destroy_process_group()
-        return
+        return run_reference(args, x, gspec, kw, config, rank, dist)
 
     import torch
     import pkde_b200 as pk
@@ -292,6 +389,20 @@ def main():
         e2e_ms = multi.max_over_ranks(e2e_ms, dist, dev)
         e2e_value = units / (e2e_ms / 1000.0)
 
+    # parity of the estimation timed first (estimation_seed(0, 0): bootstrap seed 0, the
+    # fixture's) against the FP64 oracle's committed result; recomputed here, outside the
+    # timed region (the estimation is deterministic)
+    parity = None
+    if not args.no_parity and not args.bandwidth_steps and rank == 0:
+        sys.path.insert(0, os.path.join(REPO, "tests", "golden"))
+        import config_parity as cp
+        z = cp.load(args.workload)
+        if z is not None:
+            one(multi.estimation_seed(0, 0))
+            torch.cuda.synchronize()
+            parity = cp.parity(dens.cpu().numpy(), sel.cpu().numpy(), z)
+            parity["fixture"] = os.path.basename(cp.fixture_path(args.workload))
+
     # per-phase breakdown: one more estimation with every launch timed (not in any timed region)
     _lib.get_stats(local, reset=True)
     _lib.set_profiling(_lib.PKDE_PROFILE_ALL, local)
@@ -314,12 +425,9 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl_name, "grid_points": G, "bandwidths": S, "bootstraps": B, "samples": n,
-                   "estimations_per_s": args.steps * world / (t_max / 1000.0),
-                   "p50_ms": lat_ms[len(lat_ms) // 2], "p99_ms": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))],
-                   "l2": "inputs (spectra 16(B+1)G bytes) larger than the 126 MB L2",
-                   "parallelism": f"independent estimations per rank x{world}"},
+        "dtype": "f64", "data": "synthetic", "config": config,
+        "estimations_per_s": args.steps * world / (t_max / 1000.0),
+        "p50_ms": lat_ms[len(lat_ms) // 2], "p99_ms": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))],
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(n * N * 8),
                 "d2h_bytes_per_step": int(G * 12),
                 "wall_ms_per_step": [round(v, 2) for v in e2e_walls] if e2e_value else None},
@@ -335,9 +443,15 @@ def main():
         "gpu_launches": stats["launches"],
         "clocks": clk,
     }
+    if parity is not None:
+        line["parity"] = parity
+    if not args.no_batched and args.workload == "c2" and not args.bandwidth_steps:
+        # the metric's "vs plain GPU form" part: the batched mix of 256 estimations, the same
+        # set on the plain form (one estimation per call, per-bandwidth-step launches)
+        args.steps, args.warmup = args.batched_steps, 1
+        line["batched"] = run_batched(args, world, rank, local, dist, record=True)
     if rank == 0 and not args.no_cpu_baseline and world == 1:
-        ref = cpu_reference(x, gspec, kw, budget_s=args.cpu_budget)
-        line["cpu_baseline"] = {k: ref[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line["cpu_baseline"] = cpu_baseline(x, gspec, kw, budget_s=args.cpu_budget)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -365,11 +479,12 @@ def batched_jobs(count, seed, device, torch, small=False):
     return jobs
 
 
-def run_batched(args, world, rank, local, dist):
+def run_batched(args, world, rank, local, dist, record=False):
     """--workload batched: one step = one pkde_gradepro_estimate_batch call over the whole
     set.  Also timed once each, on the same set: the plain form (one estimation per call,
     per-bandwidth-step kernel launches: the structure of the reference's CUDA path) and
-    the step engine one estimation per call."""
+    the step engine one estimation per call.  record=True (the default c2 run): the
+    configs' batched mix, returned as a dict for the main line instead of printed."""
     import torch
     import pkde_b200 as pk
     from pkde_b200 import _lib, multi, raw
@@ -377,7 +492,7 @@ def run_batched(args, world, rank, local, dist):
     dev = torch.device("cuda", local)
     pk.load()
     pk.context(local)
-    small = args.workload == "batched-small"
+    small = args.workload == "batched-small" and not record
     jobs = batched_jobs(args.batch, 3 + rank, dev, torch, small=small)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
@@ -452,7 +567,7 @@ def run_batched(args, world, rank, local, dist):
 
     # e2e: the same batch call with host samples in page-locked memory and host outputs
     e2e_value = None
-    if not args.no_e2e:
+    if not args.no_e2e and not record:
         pinned = []
         for j in jobs:
             t = torch.empty(j["host"].shape, dtype=torch.float64, pin_memory=True)
@@ -502,6 +617,15 @@ def run_batched(args, world, rank, local, dist):
         "gpu_launches": stats["launches"],
         "clocks": clk,
     }
+    if record:
+        cfg = line["config"]
+        return {"workload": cfg["workload"], "shapes": cfg["shapes"], "estimations_per_step": len(jobs),
+                "steps": args.steps, "ms_per_step": line["ms_per_step"], "estimations_per_s": est_per_s,
+                "plain_form_estimations_per_s": cfg["plain_form_estimations_per_s"],
+                "engine_one_at_a_time_estimations_per_s": cfg["engine_one_at_a_time_estimations_per_s"],
+                "batched_over_plain": cfg["batched_over_plain"], "value": value, "unit": UNIT,
+                "p50_ms_per_batch": cfg["p50_ms"], "p99_ms_per_batch": cfg["p99_ms"],
+                "roofline": line["roofline"], "gpu_launches": line["gpu_launches"], "clocks": clk}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

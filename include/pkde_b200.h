@@ -187,15 +187,20 @@ int pkde_dirac_sequence(pkde_ctx *ctx, const pkde_grid *grid, const double *data
 
 /* pkde_dirac_sequence without any device allocation.  No counterpart in the reference.
  * For callers that cannot allocate device memory: a host framework whose caching
- * allocator owns the GPU's memory, or a serving loop that must not block in
- * cudaMalloc/cudaFree, which synchronise the device.  All pointers are device pointers
- * (means_out required; sq_out, counts_out optional).  Scratch is one fixed array inside
- * the library (about 9 MB, held by every GPU that loads the library until exit):
- * at most 16384 samples per call, and when counts_out is NULL at most 2^20 resample x
- * grid-point counters.  Larger requests return PKDE_EINVAL.  The first call on a device
- * looks up the array's device address (once per device).  Calls share the array: calls
- * whose work overlaps on the GPU race; order them on one stream.  ctx may be NULL (it is
- * used only for the error message). */
+ * allocator owns the GPU's memory, or a caller that must not make cudaMalloc/cudaFree
+ * calls, which synchronise the whole device and so stall every other stream.  The call
+ * does not allocate, but it is not asynchronous: it synchronises `stream` twice (once
+ * to read back the error flags and the largest cell count, once at its end), so the
+ * calling host thread blocks until the binning has finished.  All pointers are device
+ * pointers (means_out required; sq_out, counts_out optional).  Scratch is one fixed
+ * array inside the library (about 9 MB, held by every GPU that loads the library until
+ * exit): at most 16384 samples per call, and when counts_out is NULL at most 2^20
+ * resample x grid-point counters.  Larger requests return PKDE_EINVAL.  The work runs
+ * on the device that owns `stream` (for the legacy default stream, NULL: the calling
+ * thread's current device); the pointers must belong to that device.  The first call on
+ * a device looks up the array's device address (once per device).  Calls share the
+ * array: calls whose work overlaps on the GPU race; order them on one stream.  ctx may
+ * be NULL: the error message is then kept for pkde_last_error(NULL) (per thread). */
 int pkde_dirac_sequence_noalloc(pkde_ctx *ctx, const pkde_grid *grid, const double *data, int64_t n,
                                 const int32_t *boot_idx, int32_t nboot, uint64_t seed, double *means_out,
                                 double *sq_out, uint32_t *counts_out, void *stream);
@@ -252,6 +257,36 @@ int pkde_set_step_path(pkde_ctx *ctx, int path);
  * results, only time.  On by default; 0 uses the fixed defaults (32 MB, 2 or 8 tiles,
  * delay 2).  No counterpart in the reference. */
 int pkde_set_autotune(pkde_ctx *ctx, int enable);
+
+/* Failure detection of the step engine.  Every dependency wait of the persistent
+ * step engine (a work item waiting for the items it reads from) polls a counter at most
+ * `polls` times (about 0.1 us each) before it gives up: it then sets the launch's error
+ * flag, every CTA leaves, and the call returns PKDE_ECUDA ("step engine: a dependency
+ * wait timed out").  The context stays usable.  Default 20,000,000 (about 1-2 s);
+ * polls >= 0 (0: give up at the first check that finds the dependency not ready).
+ * No counterpart in the reference, which has no waits that can time out (its
+ * failures are ArgumentErrors, DirectSpace.jl:479-512). */
+int pkde_set_wait_limit(pkde_ctx *ctx, int64_t polls);
+
+/* Host-side fault injection, for tests of the error paths (no device fault is ever
+ * made).  The next call that reaches the armed point throws a host error there and
+ * returns PKDE_ECUDA ("injected host fault"); the point then disarms itself.
+ *   PKDE_FAULT_AFTER_BINNING: in pkde_gradepro_estimate(_batch), after the binning
+ *   of every estimation and the copy of its error flags have been queued, before the
+ *   forward transforms -- the call fails with device work in flight and flags
+ *   outstanding, which the context's next call must wait for and discard.
+ * No counterpart in the reference. */
+#define PKDE_FAULT_NONE 0
+#define PKDE_FAULT_AFTER_BINNING 1
+int pkde_set_fault(pkde_ctx *ctx, int32_t point);
+
+/* Diagnostic: out[i] = num[i] / den[i] with the quotient the step engine uses for the
+ * variance-to-mean ratio (a refined hardware reciprocal estimate instead of the IEEE
+ * division subroutine), so that tests can compare it with IEEE division.  Device
+ * pointers with PKDE_DEVICE_INPUT, else host pointers.  No counterpart in the reference
+ * (whose quotient is the IEEE one, DirectSpace.jl:550-552). */
+int pkde_diag_divide(pkde_ctx *ctx, const double *num, const double *den, double *out, int64_t n, uint32_t flags,
+                     void *stream);
 
 /* Launch accounting and per-phase device time, for tracing and the roofline report.
  * No counterpart in the reference, which has no tracing.

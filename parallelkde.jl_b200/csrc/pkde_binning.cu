@@ -780,7 +780,9 @@ extern "C" int pkde_dirac_sequence(pkde_ctx *ctx, const pkde_grid *grid, const d
     using namespace pkde;
     if (!ctx) throw invalid("context is NULL");
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    settle_pending(ctx);
     cudaStream_t st = (cudaStream_t)stream;
+    DrainOnError drain{ctx, st};
     grid_validate(grid);
     if (nboot < 0) throw invalid("Number of bootstraps must be non-negative");
     if (!data) throw invalid("data is NULL");
@@ -817,9 +819,12 @@ extern "C" int pkde_dirac_sequence(pkde_ctx *ctx, const pkde_grid *grid, const d
 // Binning without device allocation (pkde_dirac_sequence_noalloc).
 //
 // For callers that cannot allocate device memory -- a host framework whose caching
-// allocator owns all of the GPU's memory, or a serving loop that must never block in
-// cudaMalloc/cudaFree (both synchronise the device).  Scratch lives in one file-scope
-// device array of fixed size; the caller passes only its input and output buffers.
+// allocator owns all of the GPU's memory, or a caller that must not call
+// cudaMalloc/cudaFree (both synchronise the whole device and stall its other streams).
+// The call itself is still blocking: it synchronises the caller's stream twice (the
+// error flags and largest count are read back between the counting and the weighting
+// phases, and the call waits for its end).  Scratch lives in one file-scope device array
+// of fixed size; the caller passes only its input and output buffers.
 // The limits below are the array's capacity.  Every call shares the array and it keeps
 // the last call's contents, so what must start at zero is cleared on each call, and two
 // calls whose work overlaps on the GPU (different streams, or host threads without
@@ -888,9 +893,22 @@ extern "C" int pkde_dirac_sequence_noalloc(pkde_ctx *ctx, const pkde_grid *grid,
       throw invalid("pkde_dirac_sequence_noalloc: %lld resample x grid counters exceed the limit %lld (pass counts_out)",
                     (long long)(nslots * G), (long long)kNoAllocMaxCounts);
     cudaStream_t st = (cudaStream_t)stream;
+    // the work runs on the device that owns the stream (the legacy default stream: the
+    // calling thread's current device), which is made current for the call
+    int dev = 0, sms = 1, prev = 0;
+    PKDE_CUDA_TRY(cudaGetDevice(&prev));
+    dev = prev;
+    if (st) PKDE_CUDA_TRY(cudaStreamGetDevice(st, &dev));
+    struct RestoreDevice {
+      int d;
+      bool on;
+      ~RestoreDevice() {
+        if (on) cudaSetDevice(d);
+      }
+    } restore{prev, dev != prev};
+    if (dev != prev) PKDE_CUDA_TRY(cudaSetDevice(dev));
+    DrainOnError drain{ctx, st};
     unsigned char *base = noalloc_scratch_for_current_device();
-    int dev = 0, sms = 1;
-    PKDE_CUDA_TRY(cudaGetDevice(&dev));
     PKDE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     uint32_t *cell = reinterpret_cast<uint32_t *>(base);
     double *rh = reinterpret_cast<double *>(base + kNoAllocCellBytes);

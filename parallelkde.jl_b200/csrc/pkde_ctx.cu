@@ -1,4 +1,5 @@
 // Context lifetime, device buffers, argument checks and small C-ABI entry points.
+#include <algorithm>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -43,6 +44,11 @@ void copy_out(void *dst, const void *src, size_t bytes, bool dst_on_device, cuda
   PKDE_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, dst_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
 }
 
+__global__ void divide_kernel(const double *num, const double *den, double *out, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = div_nr(num[i], den[i]);
+}
+
 }  // namespace pkde
 
 extern "C" {
@@ -76,7 +82,62 @@ int pkde_destroy(pkde_ctx *ctx) {
   return PKDE_OK;
 }
 
-const char *pkde_last_error(const pkde_ctx *ctx) { return ctx ? pkde::thread_error(ctx).c_str() : "no context"; }
+const char *pkde_last_error(const pkde_ctx *ctx) {
+  // NULL: the calling thread's last message of a call made without a context
+  const std::string &m = pkde::thread_error(ctx);
+  return (ctx || !m.empty()) ? m.c_str() : "no context";
+}
+
+int pkde_set_wait_limit(pkde_ctx *ctx, int64_t polls) {
+  if (!ctx) return PKDE_EINVAL;
+  if (polls < 0) {
+    pkde::thread_error(ctx) = "the wait limit must be >= 0 polls";
+    return PKDE_EINVAL;
+  }
+  ctx->wait_limit = polls;
+  return PKDE_OK;
+}
+
+int pkde_set_fault(pkde_ctx *ctx, int32_t point) {
+  if (!ctx) return PKDE_EINVAL;
+  if (point != PKDE_FAULT_NONE && point != PKDE_FAULT_AFTER_BINNING) {
+    pkde::thread_error(ctx) = "unknown fault point";
+    return PKDE_EINVAL;
+  }
+  ctx->fault_point = point;
+  return PKDE_OK;
+}
+
+int pkde_diag_divide(pkde_ctx *ctx, const double *num, const double *den, double *out, int64_t n, uint32_t flags,
+                     void *stream) {
+  return pkde_guard(ctx, [&] {
+    using namespace pkde;
+    if (!ctx) throw invalid("context is NULL");
+    if (n < 0 || (n > 0 && (!num || !den || !out))) throw invalid("num, den and out are required");
+    PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    settle_pending(ctx);
+    cudaStream_t st = (cudaStream_t)stream;
+    DrainOnError drain{ctx, st};
+    if (n == 0) return;
+    const bool dev = flags & PKDE_DEVICE_INPUT;
+    const size_t bytes = sizeof(double) * (size_t)n;
+    const double *dn = num, *dd = den;
+    double *dq = out;
+    if (!dev) {
+      double *b = (double *)ensure(ctx, BUF_MISC, 3 * bytes);
+      copy_in(b, num, bytes, false, st);
+      copy_in(b + n, den, bytes, false, st);
+      dn = b;
+      dd = b + n;
+      dq = b + 2 * n;
+    }
+    const unsigned blocks = (unsigned)std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sm_count * 8);
+    divide_kernel<<<blocks, 256, 0, st>>>(dn, dd, dq, n);
+    PKDE_CHECK_LAUNCH();
+    if (!dev) copy_out(out, dq, bytes, false, st);
+    PKDE_CUDA_TRY(cudaStreamSynchronize(st));
+  });
+}
 
 const char *pkde_version(void) { return "pkde_b200 0.1 (sm_100a, FP64 gradepro)"; }
 

@@ -21,8 +21,10 @@
 // (its state slot); the means tile t of step s needs the means tile t of step s-1
 // (convergence order).
 //
-// Memory: intermediates live in Q ring slots sized to stay in L2; data written by one
-// CTA and read by another is loaded with ld.global.cg (L2), never through L1.
+// Memory: intermediates live in Q ring slots whose size the autotuner picks per shape
+// (8-64 MB, or slots holding half or all of the bootstrap pairs: then the ring exceeds
+// the L2 and the intermediates round-trip through HBM); data written by one CTA and
+// read by another is loaded with ld.global.cg (L2), never through L1.
 #include <cuda/atomic>
 
 #include <algorithm>
@@ -50,7 +52,6 @@ template <int LOGN>
 constexpr int kEL = (1 << LOGN) / 8 >= kEngineThreads ? 1 : kEngineThreads * 8 / (1 << LOGN);
 template <int LOGN>
 using EP = Pow2<LOGN, kEL<LOGN>>;
-constexpr long long kSpinLimit = 20000000;  // ~1-2 s of polling, then the run aborts
 
 // One estimation's part of a launch (device-resident descriptor).
 struct EngineEst {
@@ -101,6 +102,7 @@ struct EngineRun {
   int64_t total_items;
   int *next;   // work counter
   int *error;  // 1: dependency wait timed out
+  long long spin_limit;  // polls per dependency wait (pkde_set_wait_limit), then the run aborts
   const double2 *tw[13];  // per-stage twiddle tables by log2(line length)
 };
 
@@ -113,11 +115,13 @@ __device__ __forceinline__ void add_release(int *p, int v) {
   a.fetch_add(v, cuda::memory_order_release);
 }
 
-// Spin until *p >= target (thread 0 only).  Returns false on timeout or abort.
-__device__ bool wait_geq(int *error, const int *p, int target) {
+// Spin until *p >= target (thread 0 only), at most `limit` polls of about 0.1 us.
+// Returns false on timeout (the launch's error flag is set) or when another CTA has
+// already aborted the launch.
+__device__ bool wait_geq(int *error, const int *p, int target, long long limit) {
   long long it = 0;
   while (ld_acquire(p) < target) {
-    if (++it > kSpinLimit || ld_acquire(error)) {
+    if (++it > limit || ld_acquire(error)) {
       atomicExch(error, 1);
       return false;
     }
@@ -194,17 +198,8 @@ __device__ void axis_tiles(double2 *smem, double2 *smem2, const double2 *sm_tw, 
   }
 }
 
-__device__ __forceinline__ double div_nr(double v, double m) {
-  double y;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(m));
-  double e = fma(-m, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-m, y, 1.0);
-  y = fma(y, e, y);
-  double q = v * y;
-  const double rem = fma(-m, q, v);
-  return fma(rem, y, q);
-}
+// VMR of one bootstrap at one point (DirectSpace.jl:550-552; 1/n as a product, the
+// quotient by div_nr).
 __device__ __forceinline__ double vmr_of(double Mv, double Vv, double inv_n) {
   const double m = fabs(Mv) * inv_n;
   const double v = fabs(Vv) * inv_n - m * m;
@@ -727,16 +722,16 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
         const int64_t s = b / (E.J + 1);
         const int j = (int)(b % (E.J + 1));
         if (p == 0) {
-          if (b >= E.Q) ok = wait_geq(R.error, E.cnt + (b - E.Q) * E.P + (E.P - 1), pass_tiles(E, b - E.Q, E.P - 1));
+          if (b >= E.Q) ok = wait_geq(R.error, E.cnt + (b - E.Q) * E.P + (E.P - 1), pass_tiles(E, b - E.Q, E.P - 1), R.spin_limit);
         } else {
-          ok = wait_geq(R.error, E.cnt + b * E.P + (p - 1), pass_tiles(E, b, p - 1));
+          ok = wait_geq(R.error, E.cnt + b * E.P + (p - 1), pass_tiles(E, b, p - 1), R.spin_limit);
         }
         if (ok && p == E.P - 1) {
-          if (j > 0) ok = wait_geq(R.error, E.fin + (b - 1) * E.Tf + s_tile, 1);  // Welford order / all groups done
+          if (j > 0) ok = wait_geq(R.error, E.fin + (b - 1) * E.Tf + s_tile, 1, R.spin_limit);  // Welford order / all groups done
           if (ok && j == 0 && s >= 2)                                                // state slot free
-            ok = wait_geq(R.error, E.fin + ((s - 2) * (E.J + 1) + E.J) * E.Tf + s_tile, 1);
+            ok = wait_geq(R.error, E.fin + ((s - 2) * (E.J + 1) + E.J) * E.Tf + s_tile, 1, R.spin_limit);
           if (ok && j == E.J && s >= 1)                                              // convergence order
-            ok = wait_geq(R.error, E.fin + ((s - 1) * (E.J + 1) + E.J) * E.Tf + s_tile, 1);
+            ok = wait_geq(R.error, E.fin + ((s - 1) * (E.J + 1) + E.J) * E.Tf + s_tile, 1, R.spin_limit);
         }
       } else {
         atomicExch(R.error, 1);  // the schedule and the descriptor disagree
@@ -1210,6 +1205,7 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
   R.total_items = total;
   R.next = (int *)(m + off_flags);
   R.error = R.next + 1;
+  R.spin_limit = (long long)ctx->wait_limit;
   bool any_gen = false;
   for (int e = 0; e < count; ++e)
     for (int j = 0; j < est[e].ndim; ++j) any_gen |= est[e].gen[j] != 0;

@@ -146,7 +146,9 @@ extern "C" int pkde_fft(pkde_ctx *ctx, int32_t ndim, const int64_t *dims, double
     if (ndim < 1 || ndim > 4 || !dims || !data || batch < 1) throw invalid("invalid FFT arguments");
     if (direction != -1 && direction != 1) throw invalid("direction must be -1 or +1");
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    settle_pending(ctx);
     cudaStream_t st = (cudaStream_t)stream;
+    DrainOnError drain{ctx, st};
     int64_t G = 1;
     for (int j = 0; j < ndim; ++j) {
       if (dims[j] < 1) throw invalid("invalid FFT size");

@@ -855,6 +855,7 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
   ctx->bin_flags = hflags;
   ctx->bin_flags_count = count;
   for (int e = 0; e < count; ++e) dirac_job_phase_b(ctx, plans[e].job, nullptr, st);
+  fault_point(ctx, PKDE_FAULT_AFTER_BINNING);
   // ---- forward FFT of every array
   for (int e = 0; e < count; ++e)
     fft_nd(ctx, plans[e].N, plans[e].g->dims, plans[e].spectra, 2 * plans[e].npairs + 1, -1, st,
@@ -1063,7 +1064,9 @@ int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradep
       if (!data[e]) throw invalid("data[%d] is NULL", e);
     }
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    settle_pending(ctx);
     cudaStream_t st = (cudaStream_t)stream;
+    DrainOnError drain{ctx, st};
     const bool din = flags & PKDE_DEVICE_INPUT, dout = flags & PKDE_DEVICE_OUTPUT;
     // host inputs: one device buffer for all samples (and one for all indices)
     std::vector<size_t> doff(count), ioff(count), ooff(count);
@@ -1108,11 +1111,6 @@ int pkde_gradepro_estimate_batch(pkde_ctx *ctx, int32_t count, const pkde_gradep
       E.d_density = dens;
       E.d_selected = sel;
     }
-    if (ctx->engine_flags_used || ctx->bin_flags_count) {  // flags left by a call that failed before its
-      PKDE_CUDA_TRY(cudaDeviceSynchronize());              // check: their copies land before reuse
-      ctx->engine_flags_used = 0;
-      ctx->bin_flags_count = 0;
-    }
     run_many(ctx, ests.data(), count, st);
     if (!dout) {
       for (int e = 0; e < count; ++e) {
@@ -1138,7 +1136,9 @@ int pkde_rot_estimate(pkde_ctx *ctx, const pkde_grid *grid, int32_t rule, const 
     if (n < 2) throw invalid("at least 2 samples are needed");
     if (!data || !density_out) throw invalid("data and density_out are required");
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    settle_pending(ctx);
     cudaStream_t st = (cudaStream_t)stream;
+    DrainOnError drain{ctx, st};
     const int N = grid->ndim;
     const int64_t G = grid_size(grid);
     const bool din = flags & PKDE_DEVICE_INPUT, dout = flags & PKDE_DEVICE_OUTPUT;
@@ -1208,7 +1208,9 @@ int pkde_scaled_vmr(pkde_ctx *ctx, int64_t G, int32_t nboot, const double *means
     if (G < 1 || nboot < 2 || ndim < 1 || ndim > 4 || !means || !sq || !t || !t0 || !vmr_out || n_samples < 1)
       throw invalid("invalid arguments to pkde_scaled_vmr");
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    settle_pending(ctx);
     cudaStream_t st = (cudaStream_t)stream;
+    DrainOnError drain{ctx, st};
     const bool din = flags & PKDE_DEVICE_INPUT, dout = flags & PKDE_DEVICE_OUTPUT;
     const size_t bytes = sizeof(double2) * G * nboot;
     const double2 *dm = (const double2 *)means, *dv = (const double2 *)sq;
@@ -1248,7 +1250,9 @@ int pkde_identify_convergence(pkde_ctx *ctx, int64_t G, double *density, const d
         !counters_over || !low_density_flags)
       throw invalid("invalid arguments to pkde_identify_convergence");
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    settle_pending(ctx);
     cudaStream_t st = (cudaStream_t)stream;
+    DrainOnError drain{ctx, st};
     const bool dev = flags & PKDE_DEVICE_INPUT;
     double *dd = density, *dmin = minima;
     const double *dmu = means, *df = vmr_current, *df1 = vmr_prev1, *df2 = vmr_prev2;

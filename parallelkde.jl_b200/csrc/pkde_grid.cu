@@ -116,7 +116,9 @@ int pkde_find_grid(pkde_ctx *ctx, int32_t ndim, const double *data, int64_t n, c
     if (ndim < 1 || ndim > 4) throw invalid("grid dimensionality must be 1..4, got %d", ndim);
     if (n < 1 || !data || !out) throw invalid("data, n >= 1 and out are required");
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    settle_pending(ctx);
     cudaStream_t st = (cudaStream_t)stream;
+    DrainOnError drain{ctx, st};
     const double *d_data = data;
     if (!(flags & PKDE_DEVICE_INPUT)) {
       double *dd = (double *)ensure(ctx, BUF_DATA, sizeof(double) * ndim * n);
@@ -174,7 +176,9 @@ int pkde_normalize_density(pkde_ctx *ctx, double *density, int64_t G, double dx,
     if (G < 1 || !density) throw invalid("density and G >= 1 are required");
     if (!(dx > 0) || !std::isfinite(dx)) throw invalid("Normalization requires a grid or dx to be specified.");
     PKDE_CUDA_TRY(cudaSetDevice(ctx->device));
+    settle_pending(ctx);
     cudaStream_t st = (cudaStream_t)stream;
+    DrainOnError drain{ctx, st};
     const bool dev = flags & PKDE_DEVICE_INPUT;
     double *d = density;
     if (!dev) {

@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <array>
+#include <exception>
 #include <map>
 #include <mutex>
 #include <string>
@@ -116,6 +117,10 @@ struct pkde_ctx {
   bool tune_wide = true;
   bool tune_loaded = false;
   std::map<std::string, std::array<int, 3>> tune;
+  // polls a step-engine dependency wait makes before it gives up (pkde_set_wait_limit)
+  int64_t wait_limit = 20000000;
+  // host-side fault injection for tests (pkde_set_fault): one-shot
+  int fault_point = PKDE_FAULT_NONE;
   // step-engine error flags, copied back without a synchronisation of their own and
   // checked when the call synchronises (check_engine_flags); page-locked
   int *engine_flags = nullptr;
@@ -588,25 +593,91 @@ void dirac_device(pkde_ctx *ctx, const pkde_grid *g, const double *d_data, int64
 }  // namespace pkde
 
 // The calling thread's last error message on a context (pkde_last_error): per thread,
-// so that threads sharing a context (pkde_submit / pkde_wait) never race on it.
+// so that threads sharing a context (pkde_submit / pkde_wait) never race on it.  Entry
+// points that accept a NULL context keep their message under the NULL key.
 namespace pkde {
 inline std::string &thread_error(const pkde_ctx *ctx) {
   thread_local std::unordered_map<const pkde_ctx *, std::string> errs;
   return errs[ctx];
 }
+
+// A call that failed after queuing work may leave device work in flight and error-flag
+// copies into page-locked memory outstanding (the flags are checked only when a call
+// reaches its final synchronisation).  Entry points that reuse the context's buffers
+// call this first: with flags outstanding it waits for the device and forgets them.
+inline void settle_pending(pkde_ctx *ctx) {
+  if (ctx->engine_flags_used || ctx->bin_flags_count) {
+    PKDE_CUDA_TRY(cudaDeviceSynchronize());
+    ctx->engine_flags_used = 0;
+    ctx->bin_flags_count = 0;
+  }
+}
+
+// Declared by an entry point once its stream is known: if the call leaves by an
+// exception, the work it already queued on that stream finishes before the error is
+// returned (so no kernel of a failed call still uses the context's buffers when the
+// caller goes on), and its outstanding error flags are discarded.
+struct DrainOnError {
+  pkde_ctx *ctx;
+  cudaStream_t st;
+  int live = std::uncaught_exceptions();
+  ~DrainOnError() {
+    if (std::uncaught_exceptions() > live) {
+      cudaStreamSynchronize(st);
+      if (ctx) {
+        ctx->engine_flags_used = 0;
+        ctx->bin_flags_count = 0;
+      }
+    }
+  }
+};
+
+// Host-side fault injection (pkde_set_fault): throws once at the armed point.
+inline void fault_point(pkde_ctx *ctx, int point) {
+  if (ctx->fault_point == point) {
+    ctx->fault_point = PKDE_FAULT_NONE;
+    throw Error{PKDE_ECUDA, "injected host fault (pkde_set_fault)"};
+  }
+}
+
+// v / m without the IEEE division subroutine: the hardware reciprocal estimate refined
+// by two Newton-Raphson iterations y <- y + y (1 - m y) (each squares the relative
+// error), the quotient q = v y, then one correction q + (v - m q) y with the exact
+// remainder from an FMA (P. Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; the same correction step
+// as in his IA-64 division).  For normal m with |m| in [2^-1020, 2^1020] and a finite
+// normal quotient the result is within 1 ulp of the IEEE quotient (2 ulp is the bound
+// the tests assert).  Elsewhere (m zero, subnormal or huge, v or the result not
+// finite) it returns the IEEE quotient v / m itself, so it never differs in kind.
+__device__ __forceinline__ double div_nr(double v, double m) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(m));
+  double e = fma(-m, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-m, y, 1.0);
+  y = fma(y, e, y);
+  const double q = v * y;
+  const double rem = fma(-m, q, v);
+  const double r = fma(rem, y, q);
+  const double am = fabs(m);
+  if (!(am >= 0x1p-1020 && am <= 0x1p1020) || !(fabs(r) <= 1.7976931348623157e308) || !(fabs(r) >= 0x1p-1022))
+    return __ddiv_rn(v, m);
+  return r;
+}
 }  // namespace pkde
 
-// Entry-point wrapper: converts exceptions into status codes + the thread's last error.
+// Entry-point wrapper: converts exceptions into status codes + the thread's last error
+// (kept under the NULL key when the call has no context).
 template <class F>
 static int pkde_guard(pkde_ctx *ctx, F &&f) {
   try {
     f();
     return PKDE_OK;
   } catch (const pkde::Error &e) {
-    if (ctx) pkde::thread_error(ctx) = e.msg;
+    pkde::thread_error(ctx) = e.msg;
     return e.code;
   } catch (const std::exception &e) {
-    if (ctx) pkde::thread_error(ctx) = e.what();
+    pkde::thread_error(ctx) = e.what();
     return PKDE_ECUDA;
   }
 }

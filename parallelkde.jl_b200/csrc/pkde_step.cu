@@ -64,22 +64,6 @@ __global__ void __launch_bounds__(Pow2<LOGN>::THREADS) axis_pass_pow2_kernel(
   for (int i = 0; i < 8; ++i) out[base + (int64_t)out_pos<LOGN>(t, i) * ls.inner] = v[i];
 }
 
-// v / m by Newton-Raphson refinement of the hardware reciprocal estimate (two
-// iterations y <- y + y (1 - m y), then one residual correction of the quotient);
-// within 2 ulp of the IEEE quotient for normal m, NaN for m == 0 (where the
-// reference's quotient is +-Inf or NaN, and both make the bootstrap variance NaN).
-__device__ __forceinline__ double div_nr(double v, double m) {
-  double y;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(m));
-  double e = fma(-m, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-m, y, 1.0);
-  y = fma(y, e, y);
-  double q = v * y;
-  const double rem = fma(-m, q, v);
-  return fma(rem, y, q);
-}
-
 // m = |M|/n, v = |V|/n - m^2, r = v/m (DirectSpace.jl:550-552; 1/n as a product).
 __device__ __forceinline__ double vmr_of(double Mv, double Vv, double inv_n) {
   const double m = fabs(Mv) * inv_n;

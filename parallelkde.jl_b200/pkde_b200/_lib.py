@@ -26,7 +26,7 @@ EXPORTED = [
     "pkde_fft", "pkde_scaled_vmr", "pkde_identify_convergence", "pkde_set_profiling", "pkde_get_stats",
     "pkde_set_step_path", "pkde_rot_estimate", "pkde_serve_config", "pkde_submit", "pkde_wait",
     "pkde_find_grid", "pkde_normalize_density", "pkde_set_autotune",
-    "pkde_boot_index",
+    "pkde_boot_index", "pkde_set_wait_limit", "pkde_set_fault", "pkde_diag_divide",
 ]
 
 PHASES = ["binning", "forward_fft", "step_fft", "step_vmr", "step_means", "other"]
@@ -94,6 +94,9 @@ def load():
     lib.pkde_normalize_density.argtypes = [vp, vp, i64, dbl, u32, vp]
     lib.pkde_rot_estimate.argtypes = [vp, ctypes.POINTER(PkdeGrid), i32, vp, i64, vp, u32, vp]
     lib.pkde_get_stats.argtypes = [vp, ctypes.POINTER(PkdeStats), ctypes.c_int]
+    lib.pkde_set_wait_limit.argtypes = [vp, i64]
+    lib.pkde_set_fault.argtypes = [vp, i32]
+    lib.pkde_diag_divide.argtypes = [vp, vp, vp, vp, i64, u32, vp]
     lib.pkde_boot_index.argtypes = [u64, i64, i64, i64]
     lib.pkde_boot_index.restype = i64
     for name in EXPORTED:
@@ -181,6 +184,37 @@ def set_autotune(enable, device=0):
     """Per-shape autotuning of the step engine's schedule (on by default)."""
     ctx = context(device)
     check(load().pkde_set_autotune(ctx, int(bool(enable))), ctx)
+
+
+DEFAULT_WAIT_LIMIT = 20_000_000
+
+
+def set_wait_limit(polls, device=0):
+    """Polls a step-engine dependency wait makes before the launch gives up (default
+    20,000,000, about 1-2 s); the call then fails with 'a dependency wait timed out'."""
+    ctx = context(device)
+    check(load().pkde_set_wait_limit(ctx, int(polls)), ctx)
+
+
+PKDE_FAULT_NONE, PKDE_FAULT_AFTER_BINNING = 0, 1
+
+
+def set_fault(point, device=0):
+    """Arm a one-shot host-side fault at `point` (tests of the error paths)."""
+    ctx = context(device)
+    check(load().pkde_set_fault(ctx, int(point)), ctx)
+
+
+def diag_divide(num, den, device=0):
+    """num / den (float64 arrays) with the quotient the step engine uses."""
+    num = np.ascontiguousarray(num, dtype=np.float64)
+    den = np.ascontiguousarray(den, dtype=np.float64)
+    if num.shape != den.shape:
+        raise ValueError("num and den must have the same shape")
+    out = np.empty_like(num)
+    ctx = context(device)
+    check(load().pkde_diag_divide(ctx, num.ctypes.data, den.ctypes.data, out.ctypes.data, num.size, 0, None), ctx)
+    return out
 
 
 def get_stats(device=0, reset=False):

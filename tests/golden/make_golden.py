@@ -9,7 +9,17 @@ agreement with the first marks the grid points whose outcome is fixed by the
 reference's arithmetic rather than by FP64 round-off.  The bootstrap draws are not
 stored: they are oracle.rng.bootstrap_indices(idx_seed, n, n_bootstraps), the same
 integer stream the CUDA library generates (pkde_boot_index).
+
+    python tests/golden/make_golden.py --configs [c1 c2 c3]
+
+makes the fixtures of the benchmarked configurations instead (config_c1/c2/c3.npz):
+the samples are not stored but regenerated from the seeded generators of
+pkde_b200.workloads (a SHA-256 of the sample bytes guards against drift), and the
+bootstrap seed is the one bench.py uses for its first timed estimation.  The 3-D
+density is stored in float32 (16 MB in float64; float32 keeps ~6e-8 relative, far
+inside the 1e-5 tolerance), selected steps in int16.
 """
+import hashlib
 import os
 import sys
 
@@ -18,6 +28,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "parallelkde.jl_b200"))
 
 from oracle import gradepro as og  # noqa: E402
 from oracle.rng import bootstrap_indices  # noqa: E402
@@ -61,6 +72,57 @@ def make(case):
     print(f"{name}: G={grid.size} S={len(ref.times)} stable={stable:.4f}")
 
 
+# The benchmarked configurations: name, workload generator, bootstrap count, bandwidth
+# steps (None: the reference's default 250), density storage type.  Bootstrap seed 0 is
+# bench.py's first timed estimation on rank 0 (multi.estimation_seed(0, 0)).
+CONFIGS = {
+    "c1": ("gaussian_1d", 100, None, np.float64),
+    "c2": ("gmm_2d", 64, 200, np.float64),
+    "c3": ("banana_t_3d", 32, 150, np.float32),
+}
+CONFIG_SEED = 0
+
+
+def config_inputs(name):
+    """Samples (N, n) and grid spec of a benchmarked configuration, regenerated."""
+    from pkde_b200 import workloads as W
+    gen, B, n_steps, _ = CONFIGS[name]
+    x, spec = getattr(W, gen)()
+    return x, spec, B, n_steps
+
+
+def sample_digest(x):
+    return hashlib.sha256(np.ascontiguousarray(x, dtype=np.float64).tobytes()).hexdigest()
+
+
+def make_config(name, workers):
+    import time
+    x, spec, B, n_steps = config_inputs(name)
+    grid = og.find_grid(x, grid_dims=spec["dims"], grid_padding=spec.get("grid_padding"))
+    idx = bootstrap_indices(CONFIG_SEED, x.shape[1], B)
+    t0 = time.time()
+    ref = og.estimate_gradepro(x, grid, idx, n_steps=n_steps, workers=workers)
+    t1 = time.time()
+    alt = og.estimate_gradepro(x, grid, idx, n_steps=n_steps, workers=workers, fft_mode="r2c")
+    t2 = time.time()
+    dt = CONFIGS[name][3]
+    rel_alt = float(np.linalg.norm(alt.density - ref.density) / np.linalg.norm(ref.density))
+    agree_alt = float(np.mean(ref.selected_step == alt.selected_step))
+    np.savez_compressed(os.path.join(HERE, f"config_{name}.npz"), workload=CONFIGS[name][0],
+                        sample_sha256=sample_digest(x), lo=grid.lo, hi=grid.hi, h=grid.h, dims=np.array(grid.dims),
+                        idx_seed=CONFIG_SEED, n_bootstraps=B, n_steps=-1 if n_steps is None else n_steps,
+                        density=ref.density.astype(dt), selected=ref.selected_step.astype(np.int16),
+                        selected_alt=alt.selected_step.astype(np.int16), rel_alt=rel_alt, agree_alt=agree_alt,
+                        oracle_seconds=t1 - t0, workers=workers)
+    print(f"config_{name}: G={grid.size} S={len(ref.times)} oracle {t1 - t0:.0f} s (r2c {t2 - t1:.0f} s) on "
+          f"{workers} threads; r2c vs c2c rel L2 {rel_alt:.2e}, agree {agree_alt:.5f}", flush=True)
+
+
 if __name__ == "__main__":
-    for c in CASES:
-        make(c)
+    if "--configs" in sys.argv:
+        names = [a for a in sys.argv[sys.argv.index("--configs") + 1:] if not a.startswith("-")] or list(CONFIGS)
+        for nm in names:
+            make_config(nm, os.cpu_count() or 1)
+    else:
+        for c in CASES:
+            make(c)

@@ -10,7 +10,9 @@ import pytest
 from oracle.rng import bootstrap_indices
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
+# the benchmarked configurations (config_*.npz) have their own tests (test_configs.py)
+FIXTURES = sorted(p for p in glob.glob(os.path.join(HERE, "golden", "*.npz"))
+                  if not os.path.basename(p).startswith("config_"))
 
 
 def load(path):

@@ -1,9 +1,9 @@
 """The allocation-free binning entry point (pkde_dirac_sequence_noalloc).
 
 It serves callers that cannot allocate device memory -- a framework whose caching
-allocator owns the GPU, or a serving loop that must not block in cudaMalloc/cudaFree,
-which synchronise the device -- by keeping its scratch in a fixed array inside the
-library.  This test calls it through the C ABI twice in a row and checks each result
+allocator owns the GPU, or a caller that must not make cudaMalloc/cudaFree calls, which
+synchronise the whole device -- by keeping its scratch in a fixed array inside the
+library (the call itself still blocks: it synchronises its stream twice).  This test calls it through the C ABI twice in a row and checks each result
 against the allocating entry point (pkde_dirac_sequence) with the tolerances of the other
 binning tests (counts bit-exact, sums within 1e-14 of the largest cell), and that device
 memory use does not change across a call.  The file name sorts last so that a run that
@@ -77,3 +77,8 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(pk):
                                          None, None)
     assert rc == _lib.PKDE_EINVAL
     assert b"16384" in lib.pkde_last_error(ctx)
+    # without a context the message is kept for pkde_last_error(NULL), per thread
+    rc = lib.pkde_dirac_sequence_noalloc(None, ctypes.byref(gs), d_data.data_ptr(), n, None, 0, 0, d_m.data_ptr(),
+                                         None, None, None)
+    assert rc == _lib.PKDE_EINVAL
+    assert b"16384" in lib.pkde_last_error(None)
