@@ -481,15 +481,29 @@ def _r2c_propagate(Mb_hat, Vb_hat, grid, t, t0):
     return Mt, Vt
 
 
+def _roundoff_noise(rng, arr, axes):
+    """Complex Gaussian noise at the round-off level of an FFT of `arr` over `axes`: per
+    array, standard deviation u sqrt(log2 G) rms(arr) with u = 2^-53 (the unit round-off),
+    the error size of a floating-point FFT (pocketfft, FFTW or this library's GPU FFT)."""
+    G = int(np.prod([arr.shape[a] for a in axes]))
+    rms = np.sqrt(np.mean(np.abs(arr) ** 2, axis=axes, keepdims=True))
+    sd = 2.0 ** -53 * math.sqrt(math.log2(max(G, 2))) * rms / math.sqrt(2.0)
+    return sd * (rng.standard_normal(arr.shape) + 1j * rng.standard_normal(arr.shape))
+
+
 def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None, alpha_s=None,
-                      alpha_os=None, eps=None, workers=1, keep_trace=False, dirac_fn=None, fft_mode="c2c"):
+                      alpha_os=None, eps=None, workers=1, keep_trace=False, dirac_fn=None, fft_mode="c2c",
+                      perturb_seed=None):
     """GradeProEstimator.jl:700-735 + :968-1060 (``estimate!``) on the CPU in FP64.
 
     data: (N, n) float64; idx: (B, n) int32 1-based bootstrap draws.
     fft_mode "c2c" follows the reference (complex transforms of the real arrays, |.| of
     the complex result); "r2c" uses real-input transforms instead -- the same
     mathematics with different FP64 rounding, used to tell which grid points' decisions
-    are decided by rounding noise (see ``stable_points``).
+    are decided by rounding noise (see ``stable_points``).  perturb_seed (c2c only) adds
+    noise of the size of FFT round-off to the forward spectra and to every inverse
+    transform's output (``_roundoff_noise``): a stand-in for another FP64 implementation,
+    whose decisions differ from the reference's exactly where rounding decides them.
     Returns GradeProResult with density/selected_step in C-order grid shape."""
     data = np.asarray(data, dtype=np.float64)
     n = data.shape[1]
@@ -505,6 +519,13 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
     Mb_hat = fourier_statistics(Mb.astype(np.complex128), workers)
     Vb_hat = fourier_statistics(Vb.astype(np.complex128), workers)
     Mf_hat = fourier_statistics(Mf.astype(np.complex128), workers)[0]
+    prng = None
+    if perturb_seed is not None:
+        prng = np.random.default_rng(perturb_seed)
+        bax = tuple(range(1, Mb_hat.ndim))
+        Mb_hat = Mb_hat + _roundoff_noise(prng, Mb_hat, bax)
+        Vb_hat = Vb_hat + _roundoff_noise(prng, Vb_hat, bax)
+        Mf_hat = Mf_hat + _roundoff_noise(prng, Mf_hat, tuple(range(Mf_hat.ndim)))
     times, steps_low, steps_over, eps = ladder(data, grid, n_steps, bw_step, bw_final, alpha_s, alpha_os, eps)
     t0 = initial_bandwidth(grid)
     t0_sq = t0 ** 2
@@ -518,8 +539,14 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
         Mt, Vt = propagate_statistics(Mb_hat, Vb_hat, grid, t, t0)
         Mt = ifourier_statistics(Mt, True, workers)
         Vt = ifourier_statistics(Vt, True, workers)
+        Ft = ifourier_statistics(propagate_means(Mf_hat, grid, t), False, workers)
+        if prng is not None:
+            bax = tuple(range(1, Mt.ndim))
+            Mt = Mt + _roundoff_noise(prng, Mt, bax)
+            Vt = Vt + _roundoff_noise(prng, Vt, bax)
+            Ft = Ft + _roundoff_noise(prng, Ft, tuple(range(Ft.ndim)))
         f = scaled_vmr(Mt, Vt, t, t0, n)
-        means = full_means(ifourier_statistics(propagate_means(Mf_hat, grid, t), False, workers))
+        means = full_means(Ft)
         dlogt = calculate_dlogt(t0_sq, t) if s == 0 else calculate_dlogt(t0_sq, t, times[s - 1])
         ms = identify_convergence(density, means, f, st.f_prev1, st.f_prev2, dlogt, st.eps, st.steps_low,
                                   st.steps_over, st.minima, st.counters_low, st.counters_over, st.low_flags)

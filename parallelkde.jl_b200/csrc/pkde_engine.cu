@@ -115,6 +115,24 @@ __device__ __forceinline__ void add_release(int *p, int v) {
   a.fetch_add(v, cuda::memory_order_release);
 }
 
+// Bring `bytes` (a multiple of 16, 16-byte aligned) at p into L2 without waiting for it
+// (bulk prefetch; no registers or shared memory involved).
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Final pass over the pairs of a batch: the z and w rows of a tile (contiguous, `tile_elems`
+// values from `first`) of pair q are fetched into L2 while pair q - 1 is transformed, so
+// that the loads of the next pair hit L2 (measured on 512 x 512 / B = 64: 5 % off the
+// engine).  Thread 0 issues it.
+__device__ __forceinline__ void prefetch_pair(const double2 *in, int64_t G, int q, int npairs, int64_t first,
+                                              int64_t tile_elems) {
+  if (threadIdx.x == 0 && q < npairs) {
+    prefetch_l2(in + (int64_t)(2 * q) * G + first, (uint32_t)(tile_elems * sizeof(double2)));
+    prefetch_l2(in + (int64_t)(2 * q + 1) * G + first, (uint32_t)(tile_elems * sizeof(double2)));
+  }
+}
+
 // Spin until *p >= target (thread 0 only), at most `limit` polls of about 0.1 us.
 // Returns false on timeout (the launch's error flag is set) or when another CTA has
 // already aborted the launch.
@@ -147,6 +165,34 @@ __host__ __device__ __forceinline__ int pass_tiles(const EngineEst &E, int64_t b
   return (int)(batch_arrays(E, b) * (E.G / E.dims[a]) / ((int64_t)E.tl[a] * E.tpi[a]));
 }
 
+// The propagation factor is separable, P(k) = prod_a f_a(k_a), and every factor but that of
+// a line's own axis is constant along the line.  So the first pass of a batch (along the
+// last axis, reading the spectra) applies all of them, with the array's scalar (1/G of the
+// inverse transform, times the second-moment scale for w arrays); the later passes load
+// their inputs as they are.
+struct PassScale {
+  const double *tab;  // the step's factor tables of the array kind (fz or fw)
+  double c;           // 1/G, times cw[s] for the second-moment arrays
+};
+
+// c times the factors of every axis but the last at line Lw of a pass-0 line set (Lw:
+// linear index over axes 1..N-1, axis 1 fastest).
+__device__ __forceinline__ double line_scale(const EngineEst &E, const PassScale &ps, int64_t Lw) {
+  double f = ps.c;
+  for (int q = 0; q < E.ndim - 1; ++q) {
+    int64_t k;
+    if (E.gen[q] == 0) {  // power-of-two axis
+      k = Lw & (E.dims[q] - 1);
+      Lw >>= E.logn[q];
+    } else {
+      k = Lw % E.dims[q];
+      Lw /= E.dims[q];
+    }
+    f *= ps.tab[E.aoff[q] + k];
+  }
+  return f;
+}
+
 // ------------------------------------------------------------------ tile bodies
 template <int LOGN>
 __device__ __forceinline__ void stage_tw(double2 *sm_tw, const double2 *tw_g, int &cached, int key) {
@@ -166,7 +212,8 @@ __device__ __forceinline__ void stage_tw(double2 *sm_tw, const double2 *tw_g, in
 // other CTAs and is read through L2 only.
 template <int LOGN, bool FROM_SPECTRA>
 __device__ void axis_tiles(double2 *smem, double2 *smem2, const double2 *sm_tw, const double2 *in, double2 *out,
-                           int64_t inner, int64_t first_tile, int ntiles, const double *f) {
+                           int64_t inner, int64_t first_tile, int ntiles, const double *f, const EngineEst &E,
+                           const PassScale ps) {
   using P = EP<LOGN>;
   using I = TileIdx<LOGN, true, kEL<LOGN>>;
   const int t = I::bfly();
@@ -181,16 +228,27 @@ __device__ void axis_tiles(double2 *smem, double2 *smem2, const double2 *sm_tw, 
       x[r] = FROM_SPECTRA ? __ldcs(in + off) : __ldcg(in + off);
     }
   };
-  // the next tile's loads are issued before this tile's FFT, hiding their latency
+  // the next tile's loads (and, in pass 0, its line scale) are issued before this tile's
+  // FFT, hiding their latency
   double2 nxt[8];
+  double ncl = 1.0;
   int64_t base = base_of(0);
   load(base, nxt);
+  if constexpr (FROM_SPECTRA) ncl = line_scale(E, ps, first_tile * P::NL + I::line());
   for (int u = 0; u < ntiles; ++u) {
     double2 v[8];
+    if constexpr (FROM_SPECTRA) {
 #pragma unroll
-    for (int r = 0; r < 8; ++r) v[r] = cscale(nxt[r], f[in_pos<LOGN>(t, r)]);
+      for (int r = 0; r < 8; ++r) v[r] = cscale(nxt[r], f[in_pos<LOGN>(t, r)] * ncl);
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r) v[r] = nxt[r];
+    }
     const int64_t nbase = u + 1 < ntiles ? base_of(u + 1) : base;
-    if (u + 1 < ntiles) load(nbase, nxt);
+    if (u + 1 < ntiles) {
+      load(nbase, nxt);
+      if constexpr (FROM_SPECTRA) ncl = line_scale(E, ps, (first_tile + u + 1) * P::NL + I::line());
+    }
     tile_fft_reg<LOGN, 1, true, kEL<LOGN>, true>(smem, v, sm_tw, smem2);
 #pragma unroll
     for (int i = 0; i < 8; ++i) __stcg(out + base + (int64_t)out_pos<LOGN>(t, i) * inner, v[i]);
@@ -213,12 +271,12 @@ __device__ __forceinline__ void welford(double x, double inv, double &mean, doub
 
 template <int LOGN>
 __device__ void vmr_tile(double2 *smem, double2 *state, double2 *sm_tw, const double2 *in, int npairs, int b0,
-                         int nboot, const double *fz, const double *fw, double cz, double cw, double inv_n, int64_t G,
-                         double *wst, int first, int64_t tile) {
+                         int nboot, double inv_n, int64_t G, double *wst, int first, int64_t tile) {
   using P = EP<LOGN>;
   using I = TileIdx<LOGN, false, kEL<LOGN>>;
   const int64_t rbase = (tile * P::NL + I::line()) * P::N;
   const int t = I::bfly();
+  prefetch_pair(in, G, 0, npairs, tile * P::NL * P::N, P::NL * P::N);
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int64_t gi = rbase + out_pos<LOGN>(t, i);
@@ -228,18 +286,13 @@ __device__ void vmr_tile(double2 *smem, double2 *state, double2 *sm_tw, const do
   for (int p = 0; p < npairs; ++p) {
     const double2 *zs = in + (int64_t)(2 * p) * G + rbase;
     const double2 *ws = zs + G;
+    prefetch_pair(in, G, p + 1, npairs, tile * P::NL * P::N, P::NL * P::N);
     double2 z[8], w[8];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int k = in_pos<LOGN>(t, r);
-      z[r] = cscale(__ldcg(zs + k), cz * fz[k]);
-    }
+    for (int r = 0; r < 8; ++r) z[r] = __ldcg(zs + in_pos<LOGN>(t, r));
     tile_fft_reg<LOGN, 1, false, kEL<LOGN>>(smem, z, sm_tw);
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-      const int k = in_pos<LOGN>(t, r);
-      w[r] = cscale(__ldcg(ws + k), cw * fw[k]);
-    }
+    for (int r = 0; r < 8; ++r) w[r] = __ldcg(ws + in_pos<LOGN>(t, r));
     tile_fft_reg<LOGN, 1, false, kEL<LOGN>>(smem, w, sm_tw);
     const int b = b0 + 2 * p;
     const double inv_a = 1.0 / (double)(b + 1), inv_b = 1.0 / (double)(b + 2);
@@ -262,19 +315,16 @@ __device__ void vmr_tile(double2 *smem, double2 *state, double2 *sm_tw, const do
 }
 
 template <int LOGN>
-__device__ void means_tile(double2 *smem, double2 *sm_tw, const double2 *in, const double *fz, double cz,
-                           const double *wst, int64_t G, int nboot, double vscale, double dlogt, double eps,
-                           int64_t steps_low, int64_t steps_over, const StepState &cs, int step, int64_t tile) {
+__device__ void means_tile(double2 *smem, double2 *sm_tw, const double2 *in, const double *wst, int64_t G, int nboot,
+                           double vscale, double dlogt, double eps, int64_t steps_low, int64_t steps_over,
+                           const StepState &cs, int step, int64_t tile) {
   using P = EP<LOGN>;
   using I = TileIdx<LOGN, false, kEL<LOGN>>;
   const int64_t rbase = (tile * P::NL + I::line()) * P::N;
   const int t = I::bfly();
   double2 z[8];
 #pragma unroll
-  for (int r = 0; r < 8; ++r) {
-    const int k = in_pos<LOGN>(t, r);
-    z[r] = cscale(__ldcg(in + rbase + k), cz * fz[k]);
-  }
+  for (int r = 0; r < 8; ++r) z[r] = __ldcg(in + rbase + in_pos<LOGN>(t, r));
   tile_fft_reg<LOGN, 1, false, kEL<LOGN>>(smem, z, sm_tw);
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
@@ -297,7 +347,7 @@ __device__ void means_tile(double2 *smem, double2 *sm_tw, const double2 *in, con
 template <bool FROM_SPECTRA>
 __device__ void axis_tiles_gen(double2 *smem, const double2 *in, double2 *out, int n, int64_t inner,
                                int64_t first_tile, int ntiles, const double *f, int TL, const FftPlan &plan,
-                               const double2 *tw) {
+                               const double2 *tw, const EngineEst &E, const PassScale ps) {
   const int pitch = n + 1;
   double2 *bufA = smem, *bufB = smem + TL * pitch;
   // TL is a power of two dividing the block size: thread i always serves line i % TL,
@@ -308,10 +358,12 @@ __device__ void axis_tiles_gen(double2 *smem, const double2 *in, double2 *out, i
   for (int u = 0; u < ntiles; ++u) {
     const int64_t L = (first_tile + u) * TL + l;
     const int64_t base = (L / inner) * n * inner + (L % inner);
+    double cl = 1.0;
+    if constexpr (FROM_SPECTRA) cl = line_scale(E, ps, L);
     for (int k = k0; k < n; k += kstep) {
       const int64_t off = base + (int64_t)k * inner;
-      const double2 x = FROM_SPECTRA ? __ldcs(in + off) : __ldcg(in + off);
-      bufA[l * pitch + k] = cscale(x, f[k]);
+      if constexpr (FROM_SPECTRA) bufA[l * pitch + k] = cscale(__ldcs(in + off), f[k] * cl);
+      else bufA[l * pitch + k] = __ldcg(in + off);
     }
     __syncthreads();
     const double2 *res = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
@@ -324,22 +376,23 @@ __device__ void axis_tiles_gen(double2 *smem, const double2 *in, double2 *out, i
 // inverse FFT of the z and w rows of every pair, VMR of both bootstraps of a pair and
 // the Welford update over bootstraps in order (state per point in shared memory).
 __device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, int npairs, int b0, int nboot,
-                             const double *fz, const double *fw, double cz, double cw, double inv_n, int64_t G,
-                             double *wst, int first, int64_t tile, int n1, int TL, const FftPlan &plan,
-                             const double2 *tw, FastDiv dn1) {
+                             double inv_n, int64_t G, double *wst, int first, int64_t tile, int n1, int TL,
+                             const FftPlan &plan, const double2 *tw, FastDiv dn1) {
   const int pitch = n1 + 1;
   double2 *bufA = smem, *bufB = smem + TL * pitch;
   const int npts = TL * n1;
   const int64_t rbase = tile * npts;
+  prefetch_pair(in, G, 0, npairs, rbase, npts);
   for (int e = threadIdx.x; e < npts; e += blockDim.x)
     state[e] = first ? make_double2(0.0, 0.0) : make_double2(__ldcg(wst + rbase + e), __ldcg(wst + G + rbase + e));
   for (int p = 0; p < npairs; ++p) {
     const double2 *zs = in + (int64_t)(2 * p) * G + rbase;
     const double2 *ws = zs + G;
+    prefetch_pair(in, G, p + 1, npairs, rbase, npts);
     double2 zval[8];
     for (int e = threadIdx.x; e < npts; e += blockDim.x) {
       const int l = (int)fdiv((uint32_t)e, dn1), k = e - l * n1;
-      bufA[l * pitch + k] = cscale(__ldcg(zs + e), cz * fz[k]);
+      bufA[l * pitch + k] = __ldcg(zs + e);
     }
     __syncthreads();
     const double2 *rz = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
@@ -351,7 +404,7 @@ __device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, i
     __syncthreads();
     for (int e = threadIdx.x; e < npts; e += blockDim.x) {
       const int l = (int)fdiv((uint32_t)e, dn1), k = e - l * n1;
-      bufA[l * pitch + k] = cscale(__ldcg(ws + e), cw * fw[k]);
+      bufA[l * pitch + k] = __ldcg(ws + e);
     }
     __syncthreads();
     const double2 *rw = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
@@ -378,17 +431,17 @@ __device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, i
   }
 }
 
-__device__ void means_tile_gen(double2 *smem, const double2 *in, const double *fz, double cz, const double *wst,
-                               int64_t G, int nboot, double vscale, double dlogt, double eps, int64_t steps_low,
-                               int64_t steps_over, const StepState &cs, int step, int64_t tile, int n1, int TL,
-                               const FftPlan &plan, const double2 *tw, FastDiv dn1) {
+__device__ void means_tile_gen(double2 *smem, const double2 *in, const double *wst, int64_t G, int nboot,
+                               double vscale, double dlogt, double eps, int64_t steps_low, int64_t steps_over,
+                               const StepState &cs, int step, int64_t tile, int n1, int TL, const FftPlan &plan,
+                               const double2 *tw, FastDiv dn1) {
   const int pitch = n1 + 1;
   double2 *bufA = smem, *bufB = smem + TL * pitch;
   const int npts = TL * n1;
   const int64_t rbase = tile * npts;
   for (int e = threadIdx.x; e < npts; e += blockDim.x) {
     const int l = (int)fdiv((uint32_t)e, dn1), k = e - l * n1;
-    bufA[l * pitch + k] = cscale(__ldcg(in + rbase + e), cz * fz[k]);
+    bufA[l * pitch + k] = __ldcg(in + rbase + e);
   }
   __syncthreads();
   const double2 *res = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
@@ -490,7 +543,8 @@ __device__ __forceinline__ bool mix_combine(const double2 *tile, const double2 *
 
 template <int R, int LM, bool FROM_SPECTRA>
 __device__ void axis_tiles_mix(double2 *tile, const double2 *sm_tw, const double2 *twc, const double2 *in,
-                               double2 *out, int64_t inner, int64_t first_tile, int ntiles, const double *f) {
+                               double2 *out, int64_t inner, int64_t first_tile, int ntiles, const double *f,
+                               const EngineEst &E, const PassScale ps) {
   using X = Mix<R, LM>;
   using T = MixTile<R, LM, X::NLA, 1>;
   const MixRole<T> ro;
@@ -501,11 +555,14 @@ __device__ void axis_tiles_mix(double2 *tile, const double2 *sm_tw, const double
     const int64_t bf = (Lf / inner) * X::N * inner + (Lf % inner);
     const int64_t bc = (Lc / inner) * X::N * inner + (Lc % inner);
     double2 v[8];
+    double cl = 1.0;
+    if constexpr (FROM_SPECTRA) cl = line_scale(E, ps, Lf);
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       const int pos = R * in_pos<LM>(ro.t, r) + ro.n1;
       const int64_t off = bf + (int64_t)pos * inner;
-      v[r] = ro.act ? cscale(FROM_SPECTRA ? __ldcs(in + off) : __ldcg(in + off), f[pos]) : make_double2(0.0, 0.0);
+      if constexpr (FROM_SPECTRA) v[r] = ro.act ? cscale(__ldcs(in + off), f[pos] * cl) : make_double2(0.0, 0.0);
+      else v[r] = ro.act ? __ldcg(in + off) : make_double2(0.0, 0.0);
     }
     mix_fft<T>(tile, sm_tw, ro, v);
 #pragma unroll
@@ -525,25 +582,25 @@ __device__ void axis_tiles_mix(double2 *tile, const double2 *sm_tw, const double
 // combine item has both transforms of its points for the VMR and the Welford update.
 template <int R, int LM>
 __device__ void vmr_tile_mix(double2 *tile, double2 *state, const double2 *sm_tw, const double2 *twc,
-                             const double2 *in, int npairs, int b0, int nboot, const double *fz, const double *fw,
-                             double cz, double cw, double inv_n, int64_t G, double *wst, int first, int64_t tile_idx) {
+                             const double2 *in, int npairs, int b0, int nboot, double inv_n, int64_t G, double *wst,
+                             int first, int64_t tile_idx) {
   using X = Mix<R, LM>;
   using T = MixTile<R, LM, X::NLF, 2>;
   const MixRole<T> ro;
   const int npts = X::NLF * X::N;
   const int64_t rbase = tile_idx * npts;
   const int lrow = (threadIdx.x % X::NLF) * X::N;
+  prefetch_pair(in, G, 0, npairs, rbase, npts);
   for (int e = threadIdx.x; e < npts; e += blockDim.x)
     state[e] = first ? make_double2(0.0, 0.0) : make_double2(__ldcg(wst + rbase + e), __ldcg(wst + G + rbase + e));
   for (int p = 0; p < npairs; ++p) {
+    prefetch_pair(in, G, p + 1, npairs, rbase, npts);
     const double2 *src = in + (int64_t)(2 * p + ro.a) * G + rbase + ro.l * X::N;
-    const double *f = ro.a ? fw : fz;
-    const double c = ro.a ? cw : cz;
     double2 v[8];
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
       const int pos = R * in_pos<LM>(ro.t, r) + ro.n1;
-      v[r] = ro.act ? cscale(__ldcg(src + pos), c * f[pos]) : make_double2(0.0, 0.0);
+      v[r] = ro.act ? __ldcg(src + pos) : make_double2(0.0, 0.0);
     }
     mix_fft<T>(tile, sm_tw, ro, v);
     const int b = b0 + 2 * p;
@@ -577,9 +634,9 @@ __device__ void vmr_tile_mix(double2 *tile, double2 *state, const double2 *sm_tw
 // Means pass over the same NLF rows (one array; the second array's threads idle).
 template <int R, int LM>
 __device__ void means_tile_mix(double2 *tile, const double2 *sm_tw, const double2 *twc, const double2 *in,
-                               const double *fz, double cz, const double *wst, int64_t G, int nboot, double vscale,
-                               double dlogt, double eps, int64_t steps_low, int64_t steps_over, const StepState &cs,
-                               int step, int64_t tile_idx) {
+                               const double *wst, int64_t G, int nboot, double vscale, double dlogt, double eps,
+                               int64_t steps_low, int64_t steps_over, const StepState &cs, int step,
+                               int64_t tile_idx) {
   using X = Mix<R, LM>;
   using T = MixTile<R, LM, X::NLF, 1>;
   const MixRole<T> ro;
@@ -590,7 +647,7 @@ __device__ void means_tile_mix(double2 *tile, const double2 *sm_tw, const double
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     const int pos = R * in_pos<LM>(ro.t, r) + ro.n1;
-    v[r] = ro.act ? cscale(__ldcg(src + pos), cz * fz[pos]) : make_double2(0.0, 0.0);
+    v[r] = ro.act ? __ldcg(src + pos) : make_double2(0.0, 0.0);
   }
   mix_fft<T>(tile, sm_tw, ro, v);
 #pragma unroll
@@ -766,30 +823,34 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
                                  : slot_base;
       in += arr * E.G;
       double2 *out = slot_base + arr * E.G;
-      const double *f = (!means && (arr & 1)) ? fws + E.aoff[a] : fzs + E.aoff[a];
-#define PKDE_AXIS(L)                                                                      \
-  {                                                                                       \
-    stage_tw<L>(sm_tw, R.tw[L], cached_tw, L);                                            \
-    if (p == 0)                                                                           \
-      axis_tiles<L, true>(tile_mem, state, sm_tw, in, out, inner, first_tile, tpi, f);    \
-    else                                                                                  \
-      axis_tiles<L, false>(tile_mem, state, sm_tw, in, out, inner, first_tile, tpi, f);   \
+      // pass 0: the line's own axis factor per element, every other factor and the array's
+      // scalar per line (PassScale); later passes apply nothing
+      const bool second = !means && (arr & 1);
+      const double *f = (second ? fws : fzs) + E.aoff[a];
+      const PassScale ps{second ? fws : fzs, second ? E.invG * E.cw[s] : E.invG};
+#define PKDE_AXIS(L)                                                                             \
+  {                                                                                              \
+    stage_tw<L>(sm_tw, R.tw[L], cached_tw, L);                                                   \
+    if (p == 0)                                                                                  \
+      axis_tiles<L, true>(tile_mem, state, sm_tw, in, out, inner, first_tile, tpi, f, E, ps);    \
+    else                                                                                         \
+      axis_tiles<L, false>(tile_mem, state, sm_tw, in, out, inner, first_tile, tpi, f, E, ps);   \
   }
-#define PKDE_AXIS_MIX(RR, LL)                                                                   \
-  {                                                                                             \
-    stage_tw<LL>(sm_tw, R.tw[LL], cached_tw, LL);                                               \
-    if (p == 0)                                                                                 \
-      axis_tiles_mix<RR, LL, true>(tile_mem, sm_tw, E.twc[a], in, out, inner, first_tile, tpi, f); \
-    else                                                                                        \
-      axis_tiles_mix<RR, LL, false>(tile_mem, sm_tw, E.twc[a], in, out, inner, first_tile, tpi, f); \
+#define PKDE_AXIS_MIX(RR, LL)                                                                             \
+  {                                                                                                       \
+    stage_tw<LL>(sm_tw, R.tw[LL], cached_tw, LL);                                                         \
+    if (p == 0)                                                                                           \
+      axis_tiles_mix<RR, LL, true>(tile_mem, sm_tw, E.twc[a], in, out, inner, first_tile, tpi, f, E, ps);  \
+    else                                                                                                  \
+      axis_tiles_mix<RR, LL, false>(tile_mem, sm_tw, E.twc[a], in, out, inner, first_tile, tpi, f, E, ps); \
   }
       if (GEN && E.gen[a] == 1) {
         if (p == 0)
           axis_tiles_gen<true>(tile_mem, in, out, (int)E.dims[a], inner, first_tile, tpi, f, E.tl[a], E.plan[a],
-                               E.twg[a]);
+                               E.twg[a], E, ps);
         else
           axis_tiles_gen<false>(tile_mem, in, out, (int)E.dims[a], inner, first_tile, tpi, f, E.tl[a], E.plan[a],
-                                E.twg[a]);
+                                E.twg[a], E, ps);
       } else if (GEN && E.gen[a] == 2) {
         PKDE_MIX_SWITCH(E.mixr[a], ln, PKDE_AXIS_MIX)
       } else {
@@ -804,23 +865,21 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
 #define PKDE_VMR(L)                                                                                         \
   {                                                                                                         \
     stage_tw<L>(sm_tw, R.tw[L], cached_tw, L);                                                              \
-    vmr_tile<L>(tile_mem, state, sm_tw, slot_base, np, 2 * j * E.g, E.nboot, fzs + E.aoff[0],               \
-                fws + E.aoff[0], E.invG, E.invG * E.cw[s], E.inv_n, E.G, E.wstate + (s & 1) * 2 * E.G,      \
-                j == 0, tile);                                                                              \
+    vmr_tile<L>(tile_mem, state, sm_tw, slot_base, np, 2 * j * E.g, E.nboot, E.inv_n, E.G,                  \
+                E.wstate + (s & 1) * 2 * E.G, j == 0, tile);                                                \
   }
 #define PKDE_VMR_MIX(RR, LL)                                                                              \
   {                                                                                                       \
     stage_tw<LL>(sm_tw, R.tw[LL], cached_tw, LL);                                                         \
-    vmr_tile_mix<RR, LL>(tile_mem, state, sm_tw, E.twc[0], slot_base, np, 2 * j * E.g, E.nboot,            \
-                         fzs + E.aoff[0], fws + E.aoff[0], E.invG, E.invG * E.cw[s], E.inv_n, E.G,         \
-                         E.wstate + (s & 1) * 2 * E.G, j == 0, tile);                                      \
+    vmr_tile_mix<RR, LL>(tile_mem, state, sm_tw, E.twc[0], slot_base, np, 2 * j * E.g, E.nboot, E.inv_n,   \
+                         E.G, E.wstate + (s & 1) * 2 * E.G, j == 0, tile);                                 \
   }
         if (GEN && E.gen[0] == 2) {
           PKDE_MIX_SWITCH(E.mixr[0], ln, PKDE_VMR_MIX)
         } else if (GEN && E.gen[0]) {
-          vmr_tile_gen(tile_mem, state, slot_base, np, 2 * j * E.g, E.nboot, fzs + E.aoff[0], fws + E.aoff[0], E.invG,
-                       E.invG * E.cw[s], E.inv_n, E.G, E.wstate + (s & 1) * 2 * E.G, j == 0, tile, (int)E.dims[0],
-                       E.tl[0], E.plan[0], E.twg[0], E.dlen[0]);
+          vmr_tile_gen(tile_mem, state, slot_base, np, 2 * j * E.g, E.nboot, E.inv_n, E.G,
+                       E.wstate + (s & 1) * 2 * E.G, j == 0, tile, (int)E.dims[0], E.tl[0], E.plan[0], E.twg[0],
+                       E.dlen[0]);
         } else {
           PKDE_ENGINE_SWITCH(ln, PKDE_VMR)
         }
@@ -830,22 +889,22 @@ __global__ void __launch_bounds__(kEngineThreads, kEngineCtas) engine_kernel(Eng
 #define PKDE_MEANS(L)                                                                                        \
   {                                                                                                          \
     stage_tw<L>(sm_tw, R.tw[L], cached_tw, L);                                                               \
-    means_tile<L>(tile_mem, sm_tw, slot_base, fzs + E.aoff[0], E.invG, E.wstate + (s & 1) * 2 * E.G, E.G,     \
-                  E.nboot, E.vscale[s], E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs, (int)s, tile);   \
+    means_tile<L>(tile_mem, sm_tw, slot_base, E.wstate + (s & 1) * 2 * E.G, E.G, E.nboot, E.vscale[s],        \
+                  E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs, (int)s, tile);                         \
   }
 #define PKDE_MEANS_MIX(RR, LL)                                                                          \
   {                                                                                                     \
     stage_tw<LL>(sm_tw, R.tw[LL], cached_tw, LL);                                                       \
-    means_tile_mix<RR, LL>(tile_mem, sm_tw, E.twc[0], slot_base, fzs + E.aoff[0], E.invG,                \
-                           E.wstate + (s & 1) * 2 * E.G, E.G, E.nboot, E.vscale[s], E.dlogt[s], E.eps,   \
-                           E.steps_low, E.steps_over, E.cs, (int)s, tile);                               \
+    means_tile_mix<RR, LL>(tile_mem, sm_tw, E.twc[0], slot_base, E.wstate + (s & 1) * 2 * E.G, E.G,      \
+                           E.nboot, E.vscale[s], E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs,     \
+                           (int)s, tile);                                                                \
   }
         if (GEN && E.gen[0] == 2) {
           PKDE_MIX_SWITCH(E.mixr[0], ln, PKDE_MEANS_MIX)
         } else if (GEN && E.gen[0]) {
-          means_tile_gen(tile_mem, slot_base, fzs + E.aoff[0], E.invG, E.wstate + (s & 1) * 2 * E.G, E.G, E.nboot,
-                         E.vscale[s], E.dlogt[s], E.eps, E.steps_low, E.steps_over, E.cs, (int)s, tile,
-                         (int)E.dims[0], E.tl[0], E.plan[0], E.twg[0], E.dlen[0]);
+          means_tile_gen(tile_mem, slot_base, E.wstate + (s & 1) * 2 * E.G, E.G, E.nboot, E.vscale[s], E.dlogt[s],
+                         E.eps, E.steps_low, E.steps_over, E.cs, (int)s, tile, (int)E.dims[0], E.tl[0], E.plan[0],
+                         E.twg[0], E.dlen[0]);
         } else {
           PKDE_ENGINE_SWITCH(ln, PKDE_MEANS)
         }

@@ -641,27 +641,29 @@ inline void fault_point(pkde_ctx *ctx, int point) {
 }
 
 // v / m without the IEEE division subroutine: the hardware reciprocal estimate refined
-// by two Newton-Raphson iterations y <- y + y (1 - m y) (each squares the relative
+// by one Newton-Raphson iteration y <- y + y (1 - m y) (which squares its relative
 // error), the quotient q = v y, then one correction q + (v - m q) y with the exact
 // remainder from an FMA (P. Markstein, "Computation of elementary functions on the IBM
 // RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; the same correction step
-// as in his IA-64 division).  For normal m with |m| in [2^-1020, 2^1020] and a finite
-// normal quotient the result is within 1 ulp of the IEEE quotient (2 ulp is the bound
-// the tests assert).  Elsewhere (m zero, subnormal or huge, v or the result not
+// as in his IA-64 division).  The correction multiplies the errors of q and y, so one
+// iteration suffices for a result within an ulp (measured against IEEE division by the
+// tests).  For |m| in [2^-1020, 2^1022) (so that 1/m is normal and
+// the estimate is not flushed) and a finite normal quotient the result is within 1 ulp of
+// the IEEE quotient (2 ulp is the bound the tests assert).  Elsewhere (m zero, subnormal or huge, v or the result not
 // finite) it returns the IEEE quotient v / m itself, so it never differs in kind.
 __device__ __forceinline__ double div_nr(double v, double m) {
   double y;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(m));
-  double e = fma(-m, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-m, y, 1.0);
+  const double e = fma(-m, y, 1.0);
   y = fma(y, e, y);
   const double q = v * y;
   const double rem = fma(-m, q, v);
   const double r = fma(rem, y, q);
-  const double am = fabs(m);
-  if (!(am >= 0x1p-1020 && am <= 0x1p1020) || !(fabs(r) <= 1.7976931348623157e308) || !(fabs(r) >= 0x1p-1022))
-    return __ddiv_rn(v, m);
+  // range tests on the biased exponents (integer pipe, not the FP64 one): |m| in
+  // [2^-1020, 2^1022) and r finite and normal, else the IEEE quotient
+  const unsigned em = ((unsigned)__double2hiint(m) >> 20) & 0x7ffu;
+  const unsigned er = ((unsigned)__double2hiint(r) >> 20) & 0x7ffu;
+  if (em - 3u > 2041u || er - 1u > 2045u) return __ddiv_rn(v, m);
   return r;
 }
 }  // namespace pkde

@@ -32,14 +32,19 @@ def samples(z):
 
 def parity(dens, sel, z):
     """Error figures of (density, selected steps) against the fixture: whole grid,
-    rounding-stable points (where the oracle's c2c and r2c runs select the same step)
-    and points where the result selects the oracle's step."""
+    rounding-stable points (where every alternative FP64 oracle run -- real-input
+    transforms, and the runs with round-off-sized perturbations when the fixture has them
+    -- selects the reference-faithful run's step) and points where the result selects
+    the oracle's step."""
     ref_d = z["density"].astype(np.float64).reshape(-1)
     ref_s = z["selected"].astype(np.int32).reshape(-1)
     alt_s = z["selected_alt"].astype(np.int32).reshape(-1)
     dens = np.asarray(dens, dtype=np.float64).reshape(-1)
     sel = np.asarray(sel).reshape(-1)
-    stable = ref_s == alt_s
+    if "unstable" in z.files:  # the ensemble of perturbed oracle runs (make_golden.py --stable)
+        stable = ~np.unpackbits(z["unstable"], count=ref_s.size).astype(bool)
+    else:
+        stable = ref_s == alt_s
     same = sel == ref_s
     both = stable & same
     nrm = lambda a: float(np.linalg.norm(a))

@@ -12,7 +12,12 @@ integer stream the CUDA library generates (pkde_boot_index).
 
     python tests/golden/make_golden.py --configs [c1 c2 c3]
 
-makes the fixtures of the benchmarked configurations instead (config_c1/c2/c3.npz):
+makes the fixtures of the benchmarked configurations instead (config_c1/c2/c3.npz), and
+
+    python tests/golden/make_golden.py --stable c2 4
+
+adds to one of them the grid points whose outcome rounding decides (an ensemble of oracle
+runs with round-off-sized perturbations; see add_stability).  The configuration fixtures:
 the samples are not stored but regenerated from the seeded generators of
 pkde_b200.workloads (a SHA-256 of the sample bytes guards against drift), and the
 bootstrap seed is the one bench.py uses for its first timed estimation.  The 3-D
@@ -118,8 +123,39 @@ def make_config(name, workers):
           f"{workers} threads; r2c vs c2c rel L2 {rel_alt:.2e}, agree {agree_alt:.5f}", flush=True)
 
 
+def add_stability(name, members, workers):
+    """Add to config_<name>.npz the grid points whose selected step depends on rounding:
+    those where any of `members` oracle runs with round-off-sized perturbations
+    (estimate_gradepro(perturb_seed=k)) or the real-input-transform run selects another
+    step than the reference-faithful run.  Stored bit-packed as `unstable`."""
+    import time
+    path = os.path.join(HERE, f"config_{name}.npz")
+    z = dict(np.load(path))
+    x, spec, B, n_steps = config_inputs(name)
+    grid = og.Grid(z["lo"], z["hi"], z["h"], tuple(int(d) for d in z["dims"]))
+    idx = bootstrap_indices(int(z["idx_seed"]), x.shape[1], B)
+    ref_sel = z["selected"].astype(np.int32).reshape(-1)
+    unstable = ref_sel != z["selected_alt"].astype(np.int32).reshape(-1)
+    agrees = []
+    for k in range(members):
+        t0 = time.time()
+        r = og.estimate_gradepro(x, grid, idx, n_steps=n_steps, workers=workers, perturb_seed=1000 + k)
+        sel = r.selected_step.reshape(-1)
+        agrees.append(float(np.mean(sel == ref_sel)))
+        unstable |= sel != ref_sel
+        print(f"config_{name}: member {k} agree {agrees[-1]:.5f}, unstable so far {np.mean(unstable):.5f} "
+              f"({time.time() - t0:.0f} s)", flush=True)
+    z["unstable"] = np.packbits(unstable)
+    z["ens_members"] = members
+    z["ens_agree"] = np.array(agrees)
+    np.savez_compressed(path, **z)
+
+
 if __name__ == "__main__":
-    if "--configs" in sys.argv:
+    if "--stable" in sys.argv:
+        i = sys.argv.index("--stable")
+        add_stability(sys.argv[i + 1], int(sys.argv[i + 2]), os.cpu_count() or 1)
+    elif "--configs" in sys.argv:
         names = [a for a in sys.argv[sys.argv.index("--configs") + 1:] if not a.startswith("-")] or list(CONFIGS)
         for nm in names:
             make_config(nm, os.cpu_count() or 1)
