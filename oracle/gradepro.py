@@ -481,29 +481,42 @@ def _r2c_propagate(Mb_hat, Vb_hat, grid, t, t0):
     return Mt, Vt
 
 
-def _roundoff_noise(rng, arr, axes):
-    """Complex Gaussian noise at the round-off level of an FFT of `arr` over `axes`: per
-    array, standard deviation u sqrt(log2 G) rms(arr) with u = 2^-53 (the unit round-off),
-    the error size of a floating-point FFT (pocketfft, FFTW or this library's GPU FFT)."""
-    G = int(np.prod([arr.shape[a] for a in axes]))
-    rms = np.sqrt(np.mean(np.abs(arr) ** 2, axis=axes, keepdims=True))
-    sd = 2.0 ** -53 * math.sqrt(math.log2(max(G, 2))) * rms / math.sqrt(2.0)
-    return sd * (rng.standard_normal(arr.shape) + 1j * rng.standard_normal(arr.shape))
+def propagator_separable(grid, t):
+    """exp(-0.5 sum_i (k_i t_i)^2) as the product of per-axis factors exp(-0.5 (k_i t_i)^2)
+    (the same mathematics, other rounding), and its square root as the product of the
+    per-axis square roots."""
+    ks = fftgrid_axes(grid)
+    p = None
+    sp = None
+    for i in range(grid.ndim):
+        e = np.exp(-0.5 * (ks[i] * t[i]) ** 2)
+        shape = [1] * grid.ndim
+        shape[grid.ndim - 1 - i] = grid.dims[i]
+        e = e.reshape(shape)
+        p = e if p is None else p * e
+        sp = np.sqrt(e) if sp is None else sp * np.sqrt(e)
+    return p, sp
 
 
 def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None, alpha_s=None,
                       alpha_os=None, eps=None, workers=1, keep_trace=False, dirac_fn=None, fft_mode="c2c",
-                      perturb_seed=None):
+                      variant=None):
     """GradeProEstimator.jl:700-735 + :968-1060 (``estimate!``) on the CPU in FP64.
 
     data: (N, n) float64; idx: (B, n) int32 1-based bootstrap draws.
     fft_mode "c2c" follows the reference (complex transforms of the real arrays, |.| of
     the complex result); "r2c" uses real-input transforms instead -- the same
     mathematics with different FP64 rounding, used to tell which grid points' decisions
-    are decided by rounding noise (see ``stable_points``).  perturb_seed (c2c only) adds
-    noise of the size of FFT round-off to the forward spectra and to every inverse
-    transform's output (``_roundoff_noise``): a stand-in for another FP64 implementation,
-    whose decisions differ from the reference's exactly where rounding decides them.
+    are decided by rounding noise (see ``stable_points``).  `variant` (c2c only) names
+    another FP64 implementation of the same mathematics, for the same purpose (each is
+    deterministic, like any real implementation):
+      "paired"     two bootstraps' real arrays in one complex transform, |Re| and |Im| as
+                   their magnitudes (the GPU library's pairing);
+      "sep"        the propagator as a product of per-axis factors (also the GPU's);
+      "paired-sep" both;
+      "longdouble" every transform and the VMR in 80-bit extended precision;
+      "jitter-K"   the forward spectra multiplied once by (1 + u g), g standard normal
+                   from seed K, u = 2^-53: the rounding of another forward transform.
     Returns GradeProResult with density/selected_step in C-order grid shape."""
     data = np.asarray(data, dtype=np.float64)
     n = data.shape[1]
@@ -516,16 +529,22 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
     if fft_mode == "r2c":
         return _estimate_r2c(data, grid, Mb, Vb, Mf, n, n_steps, bw_step, bw_final, alpha_s, alpha_os, eps,
                              workers, keep_trace)
-    Mb_hat = fourier_statistics(Mb.astype(np.complex128), workers)
-    Vb_hat = fourier_statistics(Vb.astype(np.complex128), workers)
-    Mf_hat = fourier_statistics(Mf.astype(np.complex128), workers)[0]
-    prng = None
-    if perturb_seed is not None:
-        prng = np.random.default_rng(perturb_seed)
-        bax = tuple(range(1, Mb_hat.ndim))
-        Mb_hat = Mb_hat + _roundoff_noise(prng, Mb_hat, bax)
-        Vb_hat = Vb_hat + _roundoff_noise(prng, Vb_hat, bax)
-        Mf_hat = Mf_hat + _roundoff_noise(prng, Mf_hat, tuple(range(Mf_hat.ndim)))
+    cdt = np.clongdouble if variant == "longdouble" else np.complex128
+    paired = variant in ("paired", "paired-sep")
+    if paired:  # z = M_b + i M_b+1 (odd B: the last one alone), w likewise
+        B = Mb.shape[0]
+        zs = [Mb[b] + 1j * (Mb[b + 1] if b + 1 < B else 0.0) for b in range(0, B, 2)]
+        ws = [Vb[b] + 1j * (Vb[b + 1] if b + 1 < B else 0.0) for b in range(0, B, 2)]
+        Mb_hat = fourier_statistics(np.stack(zs), workers)
+        Vb_hat = fourier_statistics(np.stack(ws), workers)
+    else:
+        Mb_hat = fourier_statistics(Mb.astype(cdt), workers)
+        Vb_hat = fourier_statistics(Vb.astype(cdt), workers)
+    Mf_hat = fourier_statistics(Mf.astype(cdt), workers)[0]
+    if variant is not None and variant.startswith("jitter-"):
+        jr = np.random.default_rng(int(variant[7:]))
+        for a in (Mb_hat, Vb_hat, Mf_hat):
+            a *= 1.0 + 2.0 ** -53 * jr.standard_normal(a.shape)
     times, steps_low, steps_over, eps = ladder(data, grid, n_steps, bw_step, bw_final, alpha_s, alpha_os, eps)
     t0 = initial_bandwidth(grid)
     t0_sq = t0 ** 2
@@ -536,17 +555,27 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
     res = GradeProResult(density, selected, times, steps_low, steps_over, eps)
     means = None
     for s, t in enumerate(times):
-        Mt, Vt = propagate_statistics(Mb_hat, Vb_hat, grid, t, t0)
+        if variant in ("sep", "paired-sep"):
+            p, sp = propagator_separable(grid, t)
+            c = _prod(t0) / math.sqrt(_prod(t0 ** 2 + t ** 2))
+            Mt = Mb_hat * p
+            Vt = Vb_hat * (sp * c)
+            Ft = Mf_hat * p
+        else:
+            Mt, Vt = propagate_statistics(Mb_hat, Vb_hat, grid, t, t0)
+            Ft = propagate_means(Mf_hat, grid, t)
         Mt = ifourier_statistics(Mt, True, workers)
         Vt = ifourier_statistics(Vt, True, workers)
-        Ft = ifourier_statistics(propagate_means(Mf_hat, grid, t), False, workers)
-        if prng is not None:
-            bax = tuple(range(1, Mt.ndim))
-            Mt = Mt + _roundoff_noise(prng, Mt, bax)
-            Vt = Vt + _roundoff_noise(prng, Vt, bax)
-            Ft = Ft + _roundoff_noise(prng, Ft, tuple(range(Ft.ndim)))
+        Ft = ifourier_statistics(Ft, False, workers)
+        if paired:  # back to one real array per bootstrap: |Re| and |Im| of each pair
+            B = Mb.shape[0]
+            Mt = np.stack([np.abs(Mt[b // 2].real if b % 2 == 0 else Mt[b // 2].imag) for b in range(B)]) + 0j
+            Vt = np.stack([np.abs(Vt[b // 2].real if b % 2 == 0 else Vt[b // 2].imag) for b in range(B)]) + 0j
         f = scaled_vmr(Mt, Vt, t, t0, n)
         means = full_means(Ft)
+        if variant == "longdouble":
+            f = f.astype(np.float64)
+            means = means.astype(np.float64)
         dlogt = calculate_dlogt(t0_sq, t) if s == 0 else calculate_dlogt(t0_sq, t, times[s - 1])
         ms = identify_convergence(density, means, f, st.f_prev1, st.f_prev2, dlogt, st.eps, st.steps_low,
                                   st.steps_over, st.minima, st.counters_low, st.counters_over, st.low_flags)

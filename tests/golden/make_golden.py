@@ -14,10 +14,10 @@ integer stream the CUDA library generates (pkde_boot_index).
 
 makes the fixtures of the benchmarked configurations instead (config_c1/c2/c3.npz), and
 
-    python tests/golden/make_golden.py --stable c2 4
+    python tests/golden/make_golden.py --stable c2 paired,sep,longdouble,jitter-1
 
-adds to one of them the grid points whose outcome rounding decides (an ensemble of oracle
-runs with round-off-sized perturbations; see add_stability).  The configuration fixtures:
+adds to one of them the grid points whose outcome rounding decides (where other FP64
+implementations of the same mathematics select another step; see add_stability).  The configuration fixtures:
 the samples are not stored but regenerated from the seeded generators of
 pkde_b200.workloads (a SHA-256 of the sample bytes guards against drift), and the
 bootstrap seed is the one bench.py uses for its first timed estimation.  The 3-D
@@ -123,11 +123,13 @@ def make_config(name, workers):
           f"{workers} threads; r2c vs c2c rel L2 {rel_alt:.2e}, agree {agree_alt:.5f}", flush=True)
 
 
-def add_stability(name, members, workers):
-    """Add to config_<name>.npz the grid points whose selected step depends on rounding:
-    those where any of `members` oracle runs with round-off-sized perturbations
-    (estimate_gradepro(perturb_seed=k)) or the real-input-transform run selects another
-    step than the reference-faithful run.  Stored bit-packed as `unstable`."""
+def add_stability(name, variants, workers):
+    """Add to config_<name>.npz the grid points whose selected step depends on FP64
+    rounding: those where any other FP64 implementation of the same mathematics -- the
+    real-input-transform run already in the fixture and the oracle's `variant`s
+    (estimate_gradepro: paired transforms, separable propagator, long double, jittered
+    forward spectra) -- selects another step than the reference-faithful run.  Stored
+    bit-packed as `unstable`, with each variant's agreement in `variant_agree`."""
     import time
     path = os.path.join(HERE, f"config_{name}.npz")
     z = dict(np.load(path))
@@ -137,24 +139,26 @@ def add_stability(name, members, workers):
     ref_sel = z["selected"].astype(np.int32).reshape(-1)
     unstable = ref_sel != z["selected_alt"].astype(np.int32).reshape(-1)
     agrees = []
-    for k in range(members):
+    for v in variants:
         t0 = time.time()
-        r = og.estimate_gradepro(x, grid, idx, n_steps=n_steps, workers=workers, perturb_seed=1000 + k)
+        r = og.estimate_gradepro(x, grid, idx, n_steps=n_steps, workers=workers, variant=v)
         sel = r.selected_step.reshape(-1)
         agrees.append(float(np.mean(sel == ref_sel)))
         unstable |= sel != ref_sel
-        print(f"config_{name}: member {k} agree {agrees[-1]:.5f}, unstable so far {np.mean(unstable):.5f} "
+        print(f"config_{name}: {v} agree {agrees[-1]:.5f}, unstable so far {np.mean(unstable):.5f} "
               f"({time.time() - t0:.0f} s)", flush=True)
-    z["unstable"] = np.packbits(unstable)
-    z["ens_members"] = members
-    z["ens_agree"] = np.array(agrees)
-    np.savez_compressed(path, **z)
+        z["unstable"] = np.packbits(unstable)
+        z["variants"] = np.array(variants[:len(agrees)])
+        z["variant_agree"] = np.array(agrees)
+        for k in ("ens_members", "ens_agree"):
+            z.pop(k, None)
+        np.savez_compressed(path, **z)
 
 
 if __name__ == "__main__":
     if "--stable" in sys.argv:
         i = sys.argv.index("--stable")
-        add_stability(sys.argv[i + 1], int(sys.argv[i + 2]), os.cpu_count() or 1)
+        add_stability(sys.argv[i + 1], sys.argv[i + 2].split(","), os.cpu_count() or 1)
     elif "--configs" in sys.argv:
         names = [a for a in sys.argv[sys.argv.index("--configs") + 1:] if not a.startswith("-")] or list(CONFIGS)
         for nm in names:
