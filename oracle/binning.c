@@ -21,6 +21,7 @@
 #include <math.h>
 #include <stdint.h>
 #include <stddef.h>
+#include <stdlib.h>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -42,9 +43,12 @@ int oracle_check_data(int ndim, const double *lo, const double *hi, const double
   return 0;
 }
 
+/* m, v: double sums (ext == 0, the reference's sequential FP64 sums) or long double sums
+ * (ext == 1: the same terms accumulated in 80-bit extended precision, later rounded once --
+ * a more exact binning, of the kind a fixed-point or compensated accumulation gives; used
+ * to tell which grid points' decisions depend on the rounding of the binned sums). */
 static void dirac_one(int ndim, const int64_t *dims, const double *lo, const double *h,
-                      const double *data, int64_t n, const int32_t *col, double *m,
-                      double *v) {
+                      const double *data, int64_t n, const int32_t *col, void *m, void *v, int ext) {
   double spacing_prod = h[0];
   for (int j = 1; j < ndim; ++j) spacing_prod = spacing_prod * h[j];
   const double spacing_squared = spacing_prod * spacing_prod;
@@ -82,10 +86,46 @@ static void dirac_one(int ndim, const int64_t *dims, const double *lo, const dou
       }
       double product = pl * ph;
       double term = product / denom;
-      m[cell] += term;
-      if (v) v[cell] += term * term;
+      if (ext) {
+        ((long double *)m)[cell] += term;
+        if (v) ((long double *)v)[cell] += term * term;
+      } else {
+        ((double *)m)[cell] += term;
+        if (v) ((double *)v)[cell] += term * term;
+      }
     }
   }
+}
+
+/* The same binning with the sums of each bootstrap column accumulated in long double and
+ * rounded to FP64 at the end (see DIRAC_ONE). */
+int oracle_dirac_ext(int ndim, const int64_t *dims, const double *lo, const double *hi,
+                     const double *h, const double *data, int64_t n, const int32_t *idx,
+                     int64_t nboot, double *means, double *sq, int nthreads) {
+  if (ndim < 1 || ndim > 4) return 3;
+  int rc = oracle_check_data(ndim, lo, hi, h, dims, data, n);
+  if (rc) return rc;
+  int64_t G = 1;
+  for (int j = 0; j < ndim; ++j) G *= dims[j];
+  for (int64_t b = 0; b < n * nboot; ++b)
+    if (idx[b] < 1 || idx[b] > n) return 4;
+#ifdef _OPENMP
+  if (nthreads < 1) nthreads = 1;
+#pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
+#endif
+  for (int64_t b = 0; b < nboot; ++b) {
+    long double *am = (long double *)calloc((size_t)G, sizeof(long double));
+    long double *av = sq ? (long double *)calloc((size_t)G, sizeof(long double)) : NULL;
+    dirac_one(ndim, dims, lo, h, data, n, idx + b * n, am, av, 1);
+    for (int64_t g = 0; g < G; ++g) {
+      means[b * G + g] = (double)am[g];
+      if (sq) sq[b * G + g] = (double)av[g];
+    }
+    free(am);
+    free(av);
+  }
+  (void)nthreads;
+  return 0;
 }
 
 /* means/sq: G x B, column-major (grid axis 1 fastest, bootstrap slowest), zeroed by the
@@ -108,7 +148,7 @@ int oracle_dirac(int ndim, const int64_t *dims, const double *lo, const double *
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1)
 #endif
   for (int64_t b = 0; b < nboot; ++b) {
-    dirac_one(ndim, dims, lo, h, data, n, idx + b * n, means + b * G, sq ? sq + b * G : NULL);
+    dirac_one(ndim, dims, lo, h, data, n, idx + b * n, means + b * G, sq ? sq + b * G : NULL, 0);
   }
   (void)nthreads;
   return 0;

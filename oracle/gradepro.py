@@ -57,11 +57,12 @@ def _lib():
         if not os.path.exists(path):
             build_oracle()
         lib = ctypes.CDLL(path)
-        lib.oracle_dirac.restype = ctypes.c_int
-        lib.oracle_dirac.argtypes = [
-            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-            ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
-            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        for fn in (lib.oracle_dirac, lib.oracle_dirac_ext):
+            fn.restype = ctypes.c_int
+            fn.argtypes = [
+                ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         _LIB = lib
     return _LIB
 
@@ -238,9 +239,11 @@ def check_data(data, grid):
             raise ValueError("Data points lie beyond grid. Remove them or increase grid boundaries.")
 
 
-def dirac(data, grid, idx, include_var=True, nthreads=1):
+def dirac(data, grid, idx, include_var=True, nthreads=1, extended=False):
     """Binning through the C restatement.  data (N, n); idx (B, n) int32 1-based.
-    Returns (M, V) real arrays of shape (B,) + grid.shape_c (V None if not include_var)."""
+    Returns (M, V) real arrays of shape (B,) + grid.shape_c (V None if not include_var).
+    extended: the same terms summed in long double and rounded once (a more exact binning
+    than the reference's sequential FP64 sums)."""
     data = np.ascontiguousarray(np.asarray(data, dtype=np.float64).T)  # (n, N) == N x n col-major
     idx = np.ascontiguousarray(idx, dtype=np.int32)
     B, n = idx.shape
@@ -250,7 +253,8 @@ def dirac(data, grid, idx, include_var=True, nthreads=1):
     M = np.zeros((B, G), dtype=np.float64)
     V = np.zeros((B, G), dtype=np.float64) if include_var else None
     dims = np.array(grid.dims, dtype=np.int64)
-    rc = _lib().oracle_dirac(grid.ndim, dims.ctypes.data, grid.lo.ctypes.data, grid.hi.ctypes.data,
+    fn = _lib().oracle_dirac_ext if extended else _lib().oracle_dirac
+    rc = fn(grid.ndim, dims.ctypes.data, grid.lo.ctypes.data, grid.hi.ctypes.data,
                              grid.h.ctypes.data, data.ctypes.data, data.shape[0], idx.ctypes.data, B,
                              M.ctypes.data, V.ctypes.data if V is not None else None, int(nthreads))
     if rc == 1:
@@ -318,9 +322,23 @@ def _spatial_axes(arr, batched):
     return tuple(range(arr.ndim - nd, arr.ndim))
 
 
+_FFT_LIB = {"lib": "pocketfft"}
+
+
+def _fftn(arr, axes, workers, inverse):
+    """scipy.fft (pocketfft), or with _FFT_LIB["lib"] == "mkl" torch's CPU FFT (Intel
+    MKL's DFT): another FP64 FFT implementation, for the rounding-stability variants."""
+    if _FFT_LIB["lib"] == "mkl" and arr.dtype == np.complex128:
+        import torch
+        t = torch.from_numpy(np.ascontiguousarray(arr))
+        out = (torch.fft.ifftn if inverse else torch.fft.fftn)(t, dim=axes)
+        return out.numpy()
+    return (sfft.ifftn if inverse else sfft.fftn)(arr, axes=axes, workers=workers)
+
+
 def fourier_statistics(arr, workers=1):
     """FourierSpace.jl:25-52: unnormalised forward FFT over the grid axes (batched)."""
-    return sfft.fftn(arr, axes=_spatial_axes(arr, True), workers=workers)
+    return _fftn(arr, _spatial_axes(arr, True), workers, False)
 
 
 def propagator(grid, t):
@@ -356,7 +374,7 @@ def propagate_means(M0, grid, t):
 
 def ifourier_statistics(arr, batched=True, workers=1):
     """FourierSpace.jl:445-472: inverse FFT scaled by 1/G."""
-    return sfft.ifftn(arr, axes=_spatial_axes(arr, batched), workers=workers)
+    return _fftn(arr, _spatial_axes(arr, batched), workers, True)
 
 
 # ------------------------------------------------------------------ direct space
@@ -516,21 +534,34 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
       "paired-sep" both;
       "longdouble" every transform and the VMR in 80-bit extended precision;
       "jitter-K"   the forward spectra multiplied once by (1 + u g), g standard normal
-                   from seed K, u = 2^-53: the rounding of another forward transform.
+                   from seed K, u = 2^-53: the rounding of another forward transform;
+      "xbin"       the binned sums accumulated in long double and rounded once (a more
+                   exact binning, like the GPU library's fixed-point sums);
+      "gpu-like"   xbin, paired and sep together;
+      "mkl", "mkl-gpu-like"  as c2c and gpu-like, every transform by Intel MKL's DFT
+                   (torch's CPU FFT) instead of pocketfft.
     Returns GradeProResult with density/selected_step in C-order grid shape."""
+    if variant is not None and variant.startswith("mkl"):
+        _FFT_LIB["lib"] = "mkl"
+        try:
+            return estimate_gradepro(data, grid, idx, n_steps, bw_step, bw_final, alpha_s, alpha_os, eps, workers,
+                                     keep_trace, dirac_fn, fft_mode, None if variant == "mkl" else variant[4:])
+        finally:
+            _FFT_LIB["lib"] = "pocketfft"
     data = np.asarray(data, dtype=np.float64)
     n = data.shape[1]
     if idx.shape[0] < 2:
         raise ValueError("at least 2 bootstraps are needed for a variance")
     binner = dirac if dirac_fn is None else dirac_fn
-    Mb, Vb = binner(data, grid, idx, include_var=True)
+    bkw = dict(extended=True, nthreads=workers) if variant in ("xbin", "gpu-like") else {}
+    Mb, Vb = binner(data, grid, idx, include_var=True, **bkw)
     ident = np.arange(1, n + 1, dtype=np.int32).reshape(1, n)
-    Mf, _ = binner(data, grid, ident, include_var=False)
+    Mf, _ = binner(data, grid, ident, include_var=False, **bkw)
     if fft_mode == "r2c":
         return _estimate_r2c(data, grid, Mb, Vb, Mf, n, n_steps, bw_step, bw_final, alpha_s, alpha_os, eps,
                              workers, keep_trace)
     cdt = np.clongdouble if variant == "longdouble" else np.complex128
-    paired = variant in ("paired", "paired-sep")
+    paired = variant in ("paired", "paired-sep", "gpu-like")
     if paired:  # z = M_b + i M_b+1 (odd B: the last one alone), w likewise
         B = Mb.shape[0]
         zs = [Mb[b] + 1j * (Mb[b + 1] if b + 1 < B else 0.0) for b in range(0, B, 2)]
@@ -555,7 +586,7 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
     res = GradeProResult(density, selected, times, steps_low, steps_over, eps)
     means = None
     for s, t in enumerate(times):
-        if variant in ("sep", "paired-sep"):
+        if variant in ("sep", "paired-sep", "gpu-like"):
             p, sp = propagator_separable(grid, t)
             c = _prod(t0) / math.sqrt(_prod(t0 ** 2 + t ** 2))
             Mt = Mb_hat * p

@@ -308,12 +308,21 @@ __global__ void resample_count_kernel(const uint32_t *__restrict__ cell_sorted, 
 
 // The quantised corner terms of DirectSpace.jl:227-237, stored at the sample's position
 // in cell order (quantize_kernel's arithmetic).
+__device__ __forceinline__ void quantize2(double v, int e, int L, unsigned long long &hi, long long &lo) {
+  // v 2^e = hi + f (hi the nearest integer, |f| <= 1/2, both exact), lo = f 2^L rounded
+  const double x = ldexp(v, e);
+  const double xr = rint(x);
+  hi = (unsigned long long)xr;
+  lo = __double2ll_rn(ldexp(x - xr, L));
+}
+
 __global__ void quantize_sorted_kernel(GridDev g, const double *__restrict__ rh, int64_t n, double denom,
                                        const int *__restrict__ esc, const uint32_t *__restrict__ pos,
-                                       unsigned long long *__restrict__ qm, unsigned long long *__restrict__ qv) {
+                                       unsigned long long *__restrict__ qm, unsigned long long *__restrict__ qv,
+                                       long long *__restrict__ qm_lo, long long *__restrict__ qv_lo) {
   int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (s >= n) return;
-  const int e_m = esc[0], e_v = esc[1];
+  const int e_m = esc[0], e_v = esc[1], L = esc[2];
   const int N = g.ndim;
   const int64_t ps = pos[s];
   double r_h[4], r_l[4];
@@ -336,8 +345,8 @@ __global__ void quantize_sorted_kernel(GridDev g, const double *__restrict__ rh,
     }
     double term = __ddiv_rn(__dmul_rn(pl, ph), denom);
     double sq = __dmul_rn(term, term);
-    qm[c * n + ps] = __double2ull_rn(ldexp(term, e_m));
-    qv[c * n + ps] = __double2ull_rn(ldexp(sq, e_v));
+    quantize2(term, e_m, L, qm[c * n + ps], qm_lo[c * n + ps]);
+    quantize2(sq, e_v, L, qv[c * n + ps], qv_lo[c * n + ps]);
   }
 }
 
@@ -349,8 +358,9 @@ template <int N>
 __global__ void weight_sorted_kernel(const uint32_t *__restrict__ cell_sorted, int64_t n, int64_t nboot, int64_t G,
                                      const int64_t *__restrict__ corner_off, const uint32_t *__restrict__ mult,
                                      const unsigned long long *__restrict__ qm,
-                                     const unsigned long long *__restrict__ qv, unsigned long long *__restrict__ out,
-                                     int64_t npairs) {
+                                     const unsigned long long *__restrict__ qv, const long long *__restrict__ qm_lo,
+                                     const long long *__restrict__ qv_lo, unsigned long long *__restrict__ out,
+                                     unsigned long long *__restrict__ out_lo, int64_t npairs) {
   constexpr int nc = 1 << N;
   const int lane = threadIdx.x & 31;
   const int64_t total = (nboot + 1) * n;
@@ -377,21 +387,33 @@ __global__ void weight_sorted_kernel(const uint32_t *__restrict__ cell_sorted, i
       const int64_t cc = (int64_t)c0 + (act ? corner_off[c] : 0);
       unsigned long long vm = m ? (unsigned long long)m * qm[c * n + i] : 0ull;
       unsigned long long vv = (m && b < nboot) ? (unsigned long long)m * qv[c * n + i] : 0ull;
+      // low parts: signed, summed modulo 2^64 (the true sums fit in 63 bits)
+      unsigned long long lm = m ? (unsigned long long)((long long)m * qm_lo[c * n + i]) : 0ull;
+      unsigned long long lv = (m && b < nboot) ? (unsigned long long)((long long)m * qv_lo[c * n + i]) : 0ull;
 #pragma unroll
       for (int k = 0; k < 5; ++k) {
         const unsigned long long um = __shfl_up_sync(0xffffffffu, vm, 1 << k);
         const unsigned long long uv = __shfl_up_sync(0xffffffffu, vv, 1 << k);
+        const unsigned long long ulm = __shfl_up_sync(0xffffffffu, lm, 1 << k);
+        const unsigned long long ulv = __shfl_up_sync(0xffffffffu, lv, 1 << k);
         if (same[k]) {
           vm += um;
           vv += uv;
+          lm += ulm;
+          lv += ulv;
         }
       }
       if (act && last) {
         if (b == nboot) {
-          if (vm) atomicAdd(&out[(2 * npairs * G + cc) * 2], vm);
+          const int64_t o = (2 * npairs * G + cc) * 2;
+          if (vm) atomicAdd(&out[o], vm);
+          if (lm) atomicAdd(&out_lo[o], lm);
         } else {
-          if (vm) atomicAdd(&out[((2 * p) * G + cc) * 2 + half], vm);
-          if (vv) atomicAdd(&out[((2 * p + 1) * G + cc) * 2 + half], vv);
+          const int64_t om = ((2 * p) * G + cc) * 2 + half, ov = ((2 * p + 1) * G + cc) * 2 + half;
+          if (vm) atomicAdd(&out[om], vm);
+          if (vv) atomicAdd(&out[ov], vv);
+          if (lm) atomicAdd(&out_lo[om], lm);
+          if (lv) atomicAdd(&out_lo[ov], lv);
         }
       }
     }
@@ -431,17 +453,25 @@ __global__ void scale_exponents_kernel(const int *misc, double nc, double tmax, 
   frexp(bv, &ex_v);
   esc[0] = 62 - ex_m;
   esc[1] = 62 - ex_v;
+  // low parts (|lo| <= 2^(L-1) a term) of at most nc * cmax terms a cell stay below 2^62
+  const unsigned long long terms = (unsigned long long)nc * (unsigned long long)(cmax > 1.0 ? cmax : 1.0);
+  const int lg = terms <= 1 ? 0 : 64 - __clzll((long long)(terms - 1));
+  esc[2] = 62 - lg;
 }
 
-// dequant_paired_kernel with the scales 2^-e_m, 2^-e_v from device memory
-__global__ void dequant_paired_esc_kernel(unsigned long long *v, int64_t G, int64_t npairs, const int *esc) {
+// Conversion of the two-part fixed-point sums to FP64, in place: hi 2^-e + lo 2^-(e+L)
+// with the exponents from device memory (w arrays use e_v).
+__global__ void dequant_paired_esc_kernel(unsigned long long *v, const unsigned long long *lo, int64_t G,
+                                          int64_t npairs, const int *esc) {
+  const int L = esc[2];
   const double sm = ldexp(1.0, -esc[0]), sv = ldexp(1.0, -esc[1]);
   const int64_t total = (2 * npairs + 1) * G * 2;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     int64_t arr = i / (2 * G);
     double sc = (arr < 2 * npairs && (arr & 1)) ? sv : sm;
-    unsigned long long x = v[i];
-    reinterpret_cast<double *>(v)[i] = (double)x * sc;
+    const unsigned long long x = v[i];
+    const double xl = (double)(long long)lo[i];
+    reinterpret_cast<double *>(v)[i] = fma(ldexp(xl, -L), sc, (double)x * sc);
   }
 }
 
@@ -592,9 +622,11 @@ size_t dirac_job_scratch(const pkde_grid *g, int64_t n, int64_t nboot) {
   const int64_t G = grid_size(g);
   const int64_t nchunk = (G + kScanChunk - 1) / kScanChunk;
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-  return al(sizeof(uint32_t) * n) + al(sizeof(double) * N * n + sizeof(unsigned long long) * 2 * nc * n) +
+  const int64_t npairs = (nboot + 1) / 2;
+  return al(sizeof(uint32_t) * n) + al(sizeof(double) * N * n + sizeof(unsigned long long) * 4 * nc * n) +
          al(sizeof(uint32_t) * (nboot + 1) * G) + 2 * al(sizeof(uint32_t) * n) + 2 * al(sizeof(uint32_t) * G) +
-         al(sizeof(uint32_t) * nchunk) + al(sizeof(uint32_t) * std::max<int64_t>(nboot, 1) * n);
+         al(sizeof(uint32_t) * nchunk) + al(sizeof(uint32_t) * std::max<int64_t>(nboot, 1) * n) +
+         al(sizeof(double2) * (2 * npairs + 1) * G);
 }
 
 void dirac_job_bind(DiracJob &j, char *scratch, int *misc) {
@@ -606,7 +638,9 @@ void dirac_job_bind(DiracJob &j, char *scratch, int *misc) {
   j.cell = (uint32_t *)scratch;
   scratch += al(sizeof(uint32_t) * j.n);
   j.rh = (double *)scratch;
-  scratch += al(sizeof(double) * N * j.n + sizeof(unsigned long long) * 2 * nc * j.n);
+  j.qm_lo = reinterpret_cast<long long *>(j.rh + N * j.n) + 2 * nc * j.n;  // after the high parts
+  j.qv_lo = j.qm_lo + nc * j.n;
+  scratch += al(sizeof(double) * N * j.n + sizeof(unsigned long long) * 4 * nc * j.n);
   j.counts = (uint32_t *)scratch;  // draws per lower cell and resample (slot nboot: identity)
   scratch += al(sizeof(uint32_t) * (j.nboot + 1) * G);
   j.pos = (uint32_t *)scratch;
@@ -620,6 +654,8 @@ void dirac_job_bind(DiracJob &j, char *scratch, int *misc) {
   j.csum = (uint32_t *)scratch;
   scratch += al(sizeof(uint32_t) * nchunk);
   j.mult = (uint32_t *)scratch;
+  scratch += al(sizeof(uint32_t) * std::max<int64_t>(j.nboot, 1) * j.n);
+  j.acc_lo = (unsigned long long *)scratch;
   j.misc = misc;
 }
 
@@ -743,18 +779,20 @@ void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
     quantize_sorted_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, st>>>(gd, j.rh, n, denom, esc,
-                                                                                            j.pos, qm, qv);
+                                                                                            j.pos, qm, qv, j.qm_lo,
+                                                                                            j.qv_lo);
   }
   PKDE_CHECK_LAUNCH();
   const int64_t npairs = (nboot + 1) / 2;
   unsigned long long *acc = reinterpret_cast<unsigned long long *>(j.paired_out);
   PKDE_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double2) * (2 * npairs + 1) * G, st));
+  PKDE_CUDA_TRY(cudaMemsetAsync(j.acc_lo, 0, sizeof(double2) * (2 * npairs + 1) * G, st));
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
     const int blocks = grid_blocks(ctx, nslots * n);
 #define PKDE_WS(NN)                                                                                          \
-  weight_sorted_kernel<NN><<<blocks, kThreads, 0, st>>>(j.cell_sorted, n, nboot, G, corner_off, j.mult, qm, qv, acc, \
-                                                        npairs)
+  weight_sorted_kernel<NN><<<blocks, kThreads, 0, st>>>(j.cell_sorted, n, nboot, G, corner_off, j.mult, qm, qv,   \
+                                                        j.qm_lo, j.qv_lo, acc, j.acc_lo, npairs)
     switch (N) {
       case 1: PKDE_WS(1); break;
       case 2: PKDE_WS(2); break;
@@ -766,7 +804,8 @@ void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_
   PKDE_CHECK_LAUNCH();
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
-    dequant_paired_esc_kernel<<<grid_blocks(ctx, (2 * npairs + 1) * G * 2), kThreads, 0, st>>>(acc, G, npairs, esc);
+    dequant_paired_esc_kernel<<<grid_blocks(ctx, (2 * npairs + 1) * G * 2), kThreads, 0, st>>>(acc, j.acc_lo, G,
+                                                                                                npairs, esc);
   }
   PKDE_CHECK_LAUNCH();
 }

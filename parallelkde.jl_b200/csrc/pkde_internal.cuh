@@ -560,6 +560,10 @@ struct DiracJob {
   uint32_t *pos = nullptr, *cell_sorted = nullptr;  // samples in lower-cell order
   uint32_t *cstart = nullptr, *cfill = nullptr, *csum = nullptr;
   uint32_t *mult = nullptr;  // nboot x n draws per sample (cell order)
+  // low parts of the two-part fixed point: per sample and corner (signed), and the sums
+  // (one 64-bit word per real value of the paired spectra)
+  long long *qm_lo = nullptr, *qv_lo = nullptr;
+  unsigned long long *acc_lo = nullptr;
   int *misc = nullptr;  // 256-byte device block
   int64_t corner_off_h[16] = {};
 };

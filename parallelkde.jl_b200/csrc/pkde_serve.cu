@@ -70,7 +70,8 @@ size_t footprint(const pkde_gradepro_params *p, int64_t n, bool has_idx) {
   b += sizeof(double2) * (2 * P + 1) * G;                                                 // spectra
   b += 64 * (size_t)G;                                                                    // state
   b += sizeof(double) * 2 * S * axes;                                                     // tables
-  b += 4 * n + 8 * N * n + 16 * nc * n + 4 * (B + 1) * G;                                 // binning
+  b += 4 * n + 8 * N * n + 32 * nc * n + 4 * (B + 1) * G;                                 // binning
+  b += sizeof(double2) * (2 * P + 1) * G;  // low parts of the fixed-point sums
   b += 4 * B * n + 8 * n + 8 * (size_t)G;  // draws per sample, cell order, cell starts
   if (N == 1) b += sizeof(double) * 2 * S * G;                                            // 1-D steps
   const size_t slot = std::max<size_t>(32u << 20, sizeof(double2) * 2 * (size_t)G);
