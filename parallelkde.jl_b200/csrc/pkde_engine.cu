@@ -82,7 +82,9 @@ struct EngineEst {
   int tl[4];                   // lines per tile, by axis
   int gen[4];                  // 1: the axis uses the shared-memory mixed-radix FFT (any length)
   const double2 *twg[4];       // generic axes: twiddle table (cos, sin)(2 pi m / n), m < n
-  FftPlan plan[4];             // generic axes: Stockham radix sequence
+  const FftPlan *plan;         // generic axes: Stockham radix sequence, by axis (device memory: the
+                               // descriptor is copied into shared memory per estimation, and the
+                               // plans are ~2 KB that only generic axes read)
   FastDiv dlen[4];             // generic axes: division by the line length
   int mixr[4];                 // mixed-radix axes (gen 2): R of N = R * 2^logn
   const double2 *twc[4];       // mixed-radix axes: combine twiddles W_N^(n1 k2), n1 = 1..R-1
@@ -1119,6 +1121,7 @@ EngineEst describe(const EngineArgs &A) {
 void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStream_t st) {
   if (count < 1) return;
   std::vector<EngineEst> est(count);
+  std::vector<std::array<FftPlan, 4>> plans(count);
   std::vector<std::vector<int64_t>> rs(count);
   size_t max_tile = 0, max_tw = 1, max_reg_tile = 0;
   EngineRun R{};
@@ -1134,7 +1137,7 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
         max_tw = std::max(max_tw, tw_elems(E.logn[j]));
       } else if (E.gen[j]) {
         E.twg[j] = twiddles_device(ctx, (int)E.dims[j]);
-        E.plan[j] = make_plan((int)E.dims[j]);
+        plans[e][j] = make_plan((int)E.dims[j]);
         E.dlen[j] = make_fastdiv((uint32_t)E.dims[j]);
         max_tile = std::max(max_tile, (size_t)2 * E.tl[j] * (size_t)(E.dims[j] + 1));
       } else {
@@ -1202,12 +1205,14 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
   const int64_t nseg = (int64_t)seg.size();
   const int64_t total = seg_start.back();
 
-  // device arena: [staged: descriptors | seg_start | seg | per estimation: scalars,
-  // round starts] [counters: per estimation cnt, fin | next, error] [per estimation:
-  // ring slots, Welford state]
+  // device arena: [staged: descriptors | FFT plans | seg_start | seg | per estimation:
+  // scalars, round starts] [counters: per estimation cnt, fin | next, error] [per
+  // estimation: ring slots, Welford state]
   size_t staged = 0;
   const size_t off_est = staged;
   staged = align256(staged + sizeof(EngineEst) * count);
+  const size_t off_plan = staged;
+  staged = align256(staged + sizeof(FftPlan) * 4 * count);
   const size_t off_segs = staged;
   staged = align256(staged + sizeof(int64_t) * (nseg + 1));
   const size_t off_seg = staged;
@@ -1244,6 +1249,8 @@ void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStre
     E.cnt = (int *)(m + off_cnt[e]);
     E.fin = E.cnt + E.NB * E.P;
     E.slots = (double2 *)(m + off_slot[e]);
+    E.plan = (const FftPlan *)(m + off_plan) + 4 * e;
+    std::memcpy(host.data() + off_plan + sizeof(FftPlan) * 4 * e, plans[e].data(), sizeof(FftPlan) * 4);
     E.wstate = (double *)(m + off_slot[e] + sizeof(double2) * (size_t)E.Q * E.slot_elems);
     double *hsc = (double *)(host.data() + off_sc[e]);
     std::memcpy(hsc, args[e].cw, sizeof(double) * E.S);
