@@ -230,27 +230,27 @@ __device__ void axis_tiles(double2 *smem, double2 *smem2, const double2 *sm_tw, 
       x[r] = FROM_SPECTRA ? __ldcs(in + off) : __ldcg(in + off);
     }
   };
-  // the next tile's loads (and, in pass 0, its line scale) are issued before this tile's
-  // FFT, hiding their latency
-  double2 nxt[8];
-  double ncl = 1.0;
+  // The next tile's rows are brought into L2 (bulk prefetch, no registers) while this tile
+  // is transformed: with its NL lines adjacent in memory (inner a multiple of NL) a tile
+  // is N segments of NL * 16 contiguous bytes.  Holding the next tile in registers instead
+  // spilled registers to local memory.
+  const bool pf = inner % P::NL == 0;
   int64_t base = base_of(0);
-  load(base, nxt);
-  if constexpr (FROM_SPECTRA) ncl = line_scale(E, ps, first_tile * P::NL + I::line());
   for (int u = 0; u < ntiles; ++u) {
     double2 v[8];
+    load(base, v);
+    if (pf && u + 1 < ntiles) {
+      const int64_t Lw0 = (first_tile + u + 1) * P::NL;
+      const int64_t b0 = (Lw0 / inner) * P::N * inner + (Lw0 % inner);
+      for (int k = threadIdx.x; k < P::N; k += kEngineThreads)
+        prefetch_l2(in + b0 + (int64_t)k * inner, (uint32_t)(P::NL * sizeof(double2)));
+    }
     if constexpr (FROM_SPECTRA) {
+      const double ncl = line_scale(E, ps, (first_tile + u) * P::NL + I::line());
 #pragma unroll
-      for (int r = 0; r < 8; ++r) v[r] = cscale(nxt[r], f[in_pos<LOGN>(t, r)] * ncl);
-    } else {
-#pragma unroll
-      for (int r = 0; r < 8; ++r) v[r] = nxt[r];
+      for (int r = 0; r < 8; ++r) v[r] = cscale(v[r], f[in_pos<LOGN>(t, r)] * ncl);
     }
     const int64_t nbase = u + 1 < ntiles ? base_of(u + 1) : base;
-    if (u + 1 < ntiles) {
-      load(nbase, nxt);
-      if constexpr (FROM_SPECTRA) ncl = line_scale(E, ps, (first_tile + u + 1) * P::NL + I::line());
-    }
     tile_fft_reg<LOGN, 1, true, kEL<LOGN>, true>(smem, v, sm_tw, smem2);
 #pragma unroll
     for (int i = 0; i < 8; ++i) __stcg(out + base + (int64_t)out_pos<LOGN>(t, i) * inner, v[i]);
