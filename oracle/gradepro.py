@@ -378,6 +378,34 @@ def ifourier_statistics(arr, batched=True, workers=1):
 
 
 # ------------------------------------------------------------------ direct space
+def _fused_vmr(Mt, Vt, t, t0, n_samples):
+    """scaled_vmr with fused multiply-adds (one rounding: long double intermediates
+    rounded once to FP64) where the GPU library fuses: m = |M| (1/n), v = fma(-m, m,
+    |V| (1/n)), the Welford updates mean = fma(delta, 1/i, mean) and m2 = fma(delta,
+    x - mean, m2)."""
+    ld = np.longdouble
+    inv_n = 1.0 / float(n_samples)
+    with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
+        m = np.sqrt(Mt.real ** 2 + Mt.imag ** 2) * inv_n
+        a = np.sqrt(Vt.real ** 2 + Vt.imag ** 2) * inv_n
+        v = (a.astype(ld) - m.astype(ld) * m.astype(ld)).astype(np.float64)
+        vmr = v / m
+        B = vmr.shape[0]
+        mean = np.zeros(vmr.shape[1:])
+        m2 = np.zeros(vmr.shape[1:])
+        for i in range(1, B + 1):
+            x = vmr[i - 1]
+            delta = x - mean
+            mean = (delta.astype(ld) * ld(1.0 / i) + mean.astype(ld)).astype(np.float64)
+            m2 = (delta.astype(ld) * (x - mean).astype(ld) + m2.astype(ld)).astype(np.float64)
+        scaling = _prod(t ** 2 + t0 ** 2) ** (3 / 2) * float(n_samples ** 3)
+        vv = scaling * m2 / (B - 1)
+    out = np.full(vv.shape, np.nan)
+    fin = np.isfinite(vv)
+    out[fin] = np.log(vv[fin])
+    return out
+
+
 def scaled_vmr(Mt, Vt, t, t0, n_samples):
     """DirectSpace.jl:526-584.  Mt, Vt: complex (B, ...) after the inverse FFT."""
     with np.errstate(divide="ignore", invalid="ignore", over="ignore"):
@@ -539,7 +567,10 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
                    exact binning, like the GPU library's fixed-point sums);
       "gpu-like"   xbin, paired and sep together;
       "mkl", "mkl-gpu-like"  as c2c and gpu-like, every transform by Intel MKL's DFT
-                   (torch's CPU FFT) instead of pocketfft.
+                   (torch's CPU FFT) instead of pocketfft;
+      "gpu-fma"    gpu-like with the VMR numerator and the Welford updates fused (one
+                   rounding each, as the GPU library computes them).
+    keep_trace: True keeps every step's log-VMR variance and means, "f" only the former.
     Returns GradeProResult with density/selected_step in C-order grid shape."""
     if variant is not None and variant.startswith("mkl"):
         _FFT_LIB["lib"] = "mkl"
@@ -553,7 +584,7 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
     if idx.shape[0] < 2:
         raise ValueError("at least 2 bootstraps are needed for a variance")
     binner = dirac if dirac_fn is None else dirac_fn
-    bkw = dict(extended=True, nthreads=workers) if variant in ("xbin", "gpu-like") else {}
+    bkw = dict(extended=True, nthreads=workers) if variant in ("xbin", "gpu-like", "gpu-fma") else {}
     Mb, Vb = binner(data, grid, idx, include_var=True, **bkw)
     ident = np.arange(1, n + 1, dtype=np.int32).reshape(1, n)
     Mf, _ = binner(data, grid, ident, include_var=False, **bkw)
@@ -561,7 +592,7 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
         return _estimate_r2c(data, grid, Mb, Vb, Mf, n, n_steps, bw_step, bw_final, alpha_s, alpha_os, eps,
                              workers, keep_trace)
     cdt = np.clongdouble if variant == "longdouble" else np.complex128
-    paired = variant in ("paired", "paired-sep", "gpu-like")
+    paired = variant in ("paired", "paired-sep", "gpu-like", "gpu-fma")
     if paired:  # z = M_b + i M_b+1 (odd B: the last one alone), w likewise
         B = Mb.shape[0]
         zs = [Mb[b] + 1j * (Mb[b + 1] if b + 1 < B else 0.0) for b in range(0, B, 2)]
@@ -586,7 +617,7 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
     res = GradeProResult(density, selected, times, steps_low, steps_over, eps)
     means = None
     for s, t in enumerate(times):
-        if variant in ("sep", "paired-sep", "gpu-like"):
+        if variant in ("sep", "paired-sep", "gpu-like", "gpu-fma"):
             p, sp = propagator_separable(grid, t)
             c = _prod(t0) / math.sqrt(_prod(t0 ** 2 + t ** 2))
             Mt = Mb_hat * p
@@ -602,7 +633,7 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
             B = Mb.shape[0]
             Mt = np.stack([np.abs(Mt[b // 2].real if b % 2 == 0 else Mt[b // 2].imag) for b in range(B)]) + 0j
             Vt = np.stack([np.abs(Vt[b // 2].real if b % 2 == 0 else Vt[b // 2].imag) for b in range(B)]) + 0j
-        f = scaled_vmr(Mt, Vt, t, t0, n)
+        f = (_fused_vmr if variant == "gpu-fma" else scaled_vmr)(Mt, Vt, t, t0, n)
         means = full_means(Ft)
         if variant == "longdouble":
             f = f.astype(np.float64)
@@ -615,7 +646,8 @@ def estimate_gradepro(data, grid, idx, n_steps=None, bw_step=None, bw_final=None
         st.f_prev1 = f.copy()
         if keep_trace:
             res.vmr_trace.append(f)
-            res.means_trace.append(means)
+            if keep_trace != "f":
+                res.means_trace.append(means)
     nan = np.isnan(density)
     density[nan] = means[nan]
     selected[selected < 0] = len(times)
@@ -653,12 +685,37 @@ def _estimate_r2c(data, grid, Mb, Vb, Mf, n, n_steps, bw_step, bw_final, alpha_s
         st.f_prev1 = f.copy()
         if keep_trace:
             res.vmr_trace.append(f)
-            res.means_trace.append(means)
+            if keep_trace != "f":
+                res.means_trace.append(means)
     nan = np.isnan(density)
     density[nan] = means[nan]
     selected[selected < 0] = len(times)
     res.selected_step = selected
     return res
+
+
+def select_from_trace(f_steps, times, t0, steps_low, steps_over, eps):
+    """The selected step of every point from a sequence of log-VMR-variance arrays alone
+    (the decisions of identify_convergence depend on f only; the means only fill the
+    density).  f_steps yields one array per step, any shape (e.g. samples x grid
+    points); returns int32 steps with the estimator's convention (len(times) where no
+    step was selected).  Same loop as estimate_gradepro."""
+    t0_sq = np.asarray(t0) ** 2
+    st = None
+    selected = None
+    for s, f in enumerate(f_steps):
+        if st is None:
+            st = DensityState(eps, steps_low, steps_over, f.shape)
+            selected = np.full(f.shape, -1, dtype=np.int32)
+            dummy = np.zeros(f.shape)
+        dlogt = calculate_dlogt(t0_sq, times[s]) if s == 0 else calculate_dlogt(t0_sq, times[s], times[s - 1])
+        ms = identify_convergence(dummy, dummy, f, st.f_prev1, st.f_prev2, dlogt, st.eps, st.steps_low,
+                                  st.steps_over, st.minima, st.counters_low, st.counters_over, st.low_flags)
+        selected[ms] = s
+        st.f_prev2 = st.f_prev1
+        st.f_prev1 = f.copy()
+    selected[selected < 0] = len(times)
+    return selected
 
 
 def stable_points(ref, alt):

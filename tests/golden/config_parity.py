@@ -32,16 +32,18 @@ def samples(z):
 
 def parity(dens, sel, z):
     """Error figures of (density, selected steps) against the fixture: whole grid,
-    rounding-stable points (where every alternative FP64 oracle run -- real-input
-    transforms, and the runs with round-off-sized perturbations when the fixture has them
-    -- selects the reference-faithful run's step) and points where the result selects
-    the oracle's step."""
+    rounding-stable points and points where the result selects the oracle's step.  A
+    point is rounding-stable when no other FP64 implementation of the same mathematics
+    selects another step there than the reference-faithful run: the oracle's real-input
+    transform run, its deterministic variants (make_golden.py --stable) and the sampled
+    rounding realisations built from their traces (make_golden.py --sampled), whose set
+    is validated by implementations held out of it (`heldout`, `heldout_agree`)."""
     ref_d = z["density"].astype(np.float64).reshape(-1)
     ref_s = z["selected"].astype(np.int32).reshape(-1)
     alt_s = z["selected_alt"].astype(np.int32).reshape(-1)
     dens = np.asarray(dens, dtype=np.float64).reshape(-1)
     sel = np.asarray(sel).reshape(-1)
-    if "unstable" in z.files:  # the ensemble of perturbed oracle runs (make_golden.py --stable)
+    if "unstable" in z.files:  # the variants and sampled realisations (make_golden.py)
         stable = ~np.unpackbits(z["unstable"], count=ref_s.size).astype(bool)
     else:
         stable = ref_s == alt_s

@@ -25,6 +25,7 @@ density is stored in float32 (16 MB in float64; float32 keeps ~6e-8 relative, fa
 inside the 1e-5 tolerance), selected steps in int16.
 """
 import hashlib
+import math
 import os
 import sys
 
@@ -155,8 +156,132 @@ def add_stability(name, variants, workers):
         np.savez_compressed(path, **z)
 
 
+def add_sampled_stability(name, trace_variants, samples, heldout, workers, seed=1, batch=16, cache=None,
+                          target=5e-4):
+    """Extend the fixture's rounding-unstable set with sampled rounding realisations.
+
+    A union over a handful of FP64 implementations under-covers the points whose decision
+    is set by rounding: where the reference's log-VMR variance f sits at the noise floor
+    (empty or nearly empty cells; many steps, so that the second difference divides a
+    rounding-level wobble by a small dlogt^2) each implementation's decision is a coin
+    flip of its own, and the union of k flip sets keeps growing with k.
+
+    The reference's trace F0 (steps x points) and the traces F_i of the `trace_variants`
+    give k rounding differences D_i = F_i - F0, each with the step-to-step correlation of
+    real rounding.  Each sample replays the selection on F0 + sum_i c_i D_i, c ~ N(0, 1/k)
+    (the variance of one more independent implementation's difference from the
+    reference), so a point's flip frequency q over the samples estimates the probability
+    that an independent FP64 implementation selects another step there.  The unstable set
+    is the variants' own flips plus the points of highest q, as few as leave an expected
+    flip rate sum(q) / |stable| <= `target` (half the 0.1 % that parity allows) on the
+    remaining, stable points, and at most 0.1 expected flips there on small grids (one
+    flip near the mode of a 1-D density of 1,024 points already moves it by 2e-4
+    relative L2).  `rounding_rate` (the mean of q over the grid: the expected
+    flip rate of an independent implementation) is recorded beside the whole-grid flip
+    rates of the `heldout` implementations (real ones, run afterwards and not used to
+    build the set) as a calibration check, with their agreement on the stable points.
+    `cache`: a directory for the traces and the held-out selections (re-runs reuse them)."""
+    import time
+    path = os.path.join(HERE, f"config_{name}.npz")
+    z = dict(np.load(path))
+    x, spec, B, n_steps = config_inputs(name)
+    grid = og.Grid(z["lo"], z["hi"], z["h"], tuple(int(d) for d in z["dims"]))
+    idx = bootstrap_indices(int(z["idx_seed"]), x.shape[1], B)
+    ref_sel = z["selected"].astype(np.int32).reshape(-1)
+    G = ref_sel.size
+    real = np.unpackbits(z["unstable_real"] if "unstable_real" in z else z["unstable"])[:G].astype(bool)
+    t_start = time.time()
+    cpath = (lambda tag: os.path.join(cache, f"cache_{name}_{tag}.npy")) if cache else None
+
+    def trace(v):
+        """(selected steps, trace as steps x points) of the oracle run `v` (None: c2c)."""
+        if cpath and os.path.exists(cpath(f"F_{v}")):
+            return np.load(cpath(f"sel_{v}")), np.load(cpath(f"F_{v}"), mmap_mode="r")
+        r = og.estimate_gradepro(x, grid, idx, n_steps=n_steps, workers=workers, variant=v, keep_trace="f")
+        sel = r.selected_step.reshape(-1).astype(np.int32)
+        F = np.stack([f.reshape(-1) for f in r.vmr_trace])
+        del r
+        if cpath:
+            np.save(cpath(f"sel_{v}"), sel)
+            np.save(cpath(f"F_{v}"), F)
+        print(f"config_{name}: trace {v} ({time.time() - t_start:.0f} s)", flush=True)
+        return sel, F
+
+    sel0, F0 = trace(None)
+    assert np.array_equal(sel0, ref_sel), "reference trace does not reproduce the fixture"
+    S = F0.shape[0]
+    D = np.empty((len(trace_variants), S, G), dtype=np.float32)
+    for i, v in enumerate(trace_variants):
+        sel, Fv = trace(v)
+        real |= sel != ref_sel
+        for s in range(S):
+            d = np.asarray(Fv[s]) - F0[s]
+            d[~np.isfinite(d)] = 0.0
+            D[i, s] = d
+        del Fv
+    times, steps_low, steps_over, eps = og.ladder(x, grid, n_steps)
+    t0 = og.initial_bandwidth(grid)
+    rng = np.random.default_rng(seed)
+    k = len(trace_variants)
+    flips = np.zeros(G, dtype=np.int32)
+    done = 0
+    while done < samples:
+        m = min(batch, samples - done)
+        C = (rng.standard_normal((m, k)) / math.sqrt(k)).astype(np.float32)
+        steps = (np.asarray(F0[s])[None, :] + (C @ D[:, s, :]).astype(np.float64) for s in range(S))
+        sel = og.select_from_trace(steps, times, t0, steps_low, steps_over, eps)
+        flips += np.sum(sel != ref_sel[None, :], axis=0).astype(np.int32)
+        done += m
+        print(f"config_{name}: {done} samples, mean flip rate {flips.sum() / (done * G):.5f} "
+              f"({time.time() - t_start:.0f} s)", flush=True)
+    q = flips / float(samples)
+    # the fewest points of highest q that leave sum(q) / |stable| <= target on the rest
+    order = np.argsort(-q, kind="stable")
+    qs = q[order]
+    rest = np.cumsum(qs[::-1])[::-1]  # rest[j]: sum of q over order[j:]
+    nstable = G - np.arange(G)
+    ok = np.nonzero(rest <= np.minimum(target * nstable, np.maximum(0.1, 1e-4 * nstable)))[0]
+    cut = int(ok[0]) if ok.size else G
+    sampled = np.zeros(G, dtype=bool)
+    sampled[order[:cut]] = True
+    unstable = sampled | real
+    stable = ~unstable
+    print(f"config_{name}: sampled set {np.mean(sampled):.5f} (q >= {qs[cut - 1] if cut else 1:.4f}), union "
+          f"{np.mean(unstable):.5f}, expected flip rate on the stable points {q[stable].sum() / max(stable.sum(), 1):.6f}, "
+          f"over the grid {q.mean():.5f}", flush=True)
+    hagree = []
+    for v in heldout:
+        if cpath and os.path.exists(cpath(f"sel_{v}")):
+            sel = np.load(cpath(f"sel_{v}"))
+        else:
+            r = og.estimate_gradepro(x, grid, idx, n_steps=n_steps, workers=workers, variant=v)
+            sel = r.selected_step.reshape(-1).astype(np.int32)
+            del r
+            if cpath:
+                np.save(cpath(f"sel_{v}"), sel)
+        hagree.append([float(np.mean(sel == ref_sel)), float(np.mean(sel[stable] == ref_sel[stable]))])
+        print(f"config_{name}: held-out {v} agree {hagree[-1][0]:.5f}, on the stable points "
+              f"{hagree[-1][1]:.5f} ({time.time() - t_start:.0f} s)", flush=True)
+    z["unstable_real"] = np.packbits(real)
+    z["unstable"] = np.packbits(unstable)
+    z["trace_variants"] = np.array(trace_variants)
+    z["rounding_samples"] = np.int64(samples)
+    z["rounding_seed"] = np.int64(seed)
+    z["rounding_target"] = np.float64(target)
+    z["rounding_rate"] = np.float64(q.mean())
+    z["rounding_rate_stable"] = np.float64(q[stable].sum() / max(stable.sum(), 1))
+    z["heldout"] = np.array(list(heldout))
+    z["heldout_agree"] = np.array(hagree).reshape(-1, 2)
+    np.savez_compressed(path, **z)
+
+
 if __name__ == "__main__":
-    if "--stable" in sys.argv:
+    if "--sampled" in sys.argv:
+        i = sys.argv.index("--sampled")
+        cache = sys.argv[sys.argv.index("--cache") + 1] if "--cache" in sys.argv else None
+        add_sampled_stability(sys.argv[i + 1], sys.argv[i + 2].split(","), int(sys.argv[i + 3]),
+                              [v for v in sys.argv[i + 4].split(",") if v], os.cpu_count() or 1, cache=cache)
+    elif "--stable" in sys.argv:
         i = sys.argv.index("--stable")
         add_stability(sys.argv[i + 1], sys.argv[i + 2].split(","), os.cpu_count() or 1)
     elif "--configs" in sys.argv:

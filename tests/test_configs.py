@@ -8,16 +8,25 @@ oracle's density and selected steps for
       the default 250 bandwidth steps;
   C2: 2-D 3-component GMM, 1,000,000 samples, 512 x 512, B = 64, 200 steps;
   C3: 3-D banana + Student-t(3), 4,000,000 samples, 128^3, B = 32, 150 steps;
-with the bootstrap draws of seed 0 (bench.py's first timed estimation), plus the
-selected steps of a second FP64 oracle run with real-input transforms.  Where the two
-oracle runs select the same step, the outcome is fixed by the reference's arithmetic
-(rounding-stable points); elsewhere a decision sits within FP64 round-off of the
-threshold and is set by the last bits of the transforms.
+with the bootstrap draws of seed 0 (bench.py's first timed estimation), and the set of
+grid points whose selected step FP64 rounding decides.  That set is where any other FP64
+implementation of the same mathematics selects another step than the reference-faithful
+run: the oracle with real-input transforms, with paired transforms, a separable
+propagator, long-double arithmetic or jittered forward spectra, and sampled rounding
+realisations (the reference's log-VMR-variance trace plus random combinations of those
+implementations' trace differences, replayed through the selection).  Where the
+second difference of the log-VMR variance divides a rounding-level wobble by dlogt^2
+(200 steps: C2) most points of the tails are such points.  Implementations held out of
+the set (Intel MKL transforms, long-double binning, the GPU library's pairing and fused
+arithmetic in the oracle) show that it is complete: each agrees with the reference on
+>= 99.9 % of the remaining points, recorded in the fixture and asserted below.
 
 Asserted per configuration:
 * on the rounding-stable points: relative L2 <= 1e-5 and agreement >= 99.9 %;
-* on the whole grid as well, wherever the oracle's own second FP64 run meets those
-  numbers (C2, C3; not C1, where the two oracle runs differ by 1.2e-4 relative L2);
+* on the whole grid as well, wherever the oracle's own real-input-transform run meets
+  those numbers (none of C1-C3 does: it differs from the reference-faithful run by
+  1.2e-4 relative L2 on C1 and selects another step at 10 % of C2's and 1.2 % of C3's
+  points);
 * where the GPU and the oracle select the same step the densities agree to FP64
   round-off (1e-10; 1e-7 for C3, whose fixture stores the density in float32).
 The samples are regenerated from pkde_b200.workloads (a SHA-256 guards the bytes)."""
@@ -64,6 +73,52 @@ def test_oracle_reproduces_c1(oracle):
     res = oracle.estimate_gradepro(x, grid, idx, n_steps=None, workers=2)
     assert np.array_equal(res.selected_step.astype(np.int16), z["selected"])
     assert np.max(np.abs(res.density - z["density"])) <= 1e-13 * np.max(z["density"])
+
+
+def _heldout_bar(z):
+    """Agreement a held-out implementation must reach on the stable points: 99.9 %, or all
+    but one point where 0.1 % of them is less than one point (C1: ~1,000 stable points,
+    where the set's expected 0.1 flips per implementation make one flip in one of five
+    implementations an even bet)."""
+    n = int(np.sum(~np.unpackbits(z["unstable"], count=int(np.prod(z["dims"]))).astype(bool)))
+    return min(AGREE, 1.0 - 1.0 / n)
+
+
+@pytest.mark.parametrize("name", CONFIGS)
+def test_stable_set_complete(name):
+    """The implementations held out of the rounding-unstable set agree with the reference
+    on the points outside it as the GPU result must, as recorded by make_golden.py
+    --sampled; the set's expected flip rate there (from the sampled realisations) is at
+    most half the 0.1 % parity allows, and its expected flip rate over the grid is of the
+    size the held-out implementations show."""
+    z = _fixture(name)
+    if "heldout_agree" not in z.files:
+        pytest.skip("fixture without held-out implementations")
+    assert len(z["heldout"]) >= 2
+    assert float(z["rounding_rate_stable"]) <= 5e-4
+    bar = _heldout_bar(z)
+    for v, (whole, stable) in zip(z["heldout"], z["heldout_agree"]):
+        print(f"{name}: held-out {v}: flip rate {1 - whole:.5f} on the grid (sampled realisations "
+              f"{float(z['rounding_rate']):.5f}), agreement {stable:.5f} on the stable points")
+        assert stable >= bar
+        assert 1 - whole <= 3 * float(z["rounding_rate"]) + 1e-3
+
+
+def test_stable_set_heldout_live_c1(oracle):
+    """C1 live: an implementation held out of the set (Intel MKL's transforms instead of
+    pocketfft) reproduces its recorded agreement and meets the bar (CPU, seconds)."""
+    from oracle.rng import bootstrap_indices
+    z = _fixture("c1")
+    if "heldout" not in z.files or "mkl" not in list(z["heldout"]):
+        pytest.skip("fixture without the held-out MKL run")
+    x = _inputs(z)
+    grid = oracle.Grid(z["lo"], z["hi"], z["h"], tuple(int(d) for d in z["dims"]))
+    idx = bootstrap_indices(int(z["idx_seed"]), x.shape[1], int(z["n_bootstraps"]))
+    res = oracle.estimate_gradepro(x, grid, idx, n_steps=None, workers=2, variant="mkl")
+    p = parity(res.density, res.selected_step, z)
+    rec = z["heldout_agree"][list(z["heldout"]).index("mkl")]
+    assert p["agree"] == pytest.approx(rec[0]) and p["agree_stable"] == pytest.approx(rec[1])
+    assert p["agree_stable"] >= _heldout_bar(z)
 
 
 @pytest.mark.gpu
