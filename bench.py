@@ -281,6 +281,8 @@ def main():
     ap.add_argument("--no-serial", action="store_true", help="--impl reference: skip the 1-thread sample")
     ap.add_argument("--bandwidth-steps", type=int, default=None,
                     help="override the workload's bandwidth steps (small profiling runs only)")
+    ap.add_argument("--bootstraps", type=int, default=None,
+                    help="override the workload's bootstrap count (small profiling runs only)")
     args = ap.parse_args()
     world, rank, local, dist = dist_setup(args)
     if args.workload in ("batched", "batched-small", "served") and args.impl == "reference":
@@ -297,9 +299,15 @@ def main():
     x, gspec, kw = workload(args.workload)
     if args.bandwidth_steps:
         kw["n_steps"] = args.bandwidth_steps
+    if args.bootstraps:
+        kw["n_bootstraps"] = args.bootstraps
+    small = bool(args.bandwidth_steps or args.bootstraps)  # a profiling case, not the workload
     wl_name = {"c1": "1-D N(0,1) n=1e4, 1024 pts, B=100, 251 bandwidths",
                "c2": "2-D 3-GMM n=1e6, 512x512, B=64, 201 bandwidths",
                "c3": "3-D banana+t3 n=4e6, 128^3, B=32, 151 bandwidths"}[args.workload]
+    if small:
+        wl_name = (f"profiling case of {args.workload} ({wl_name.split(',')[0]}): B={kw['n_bootstraps']}, "
+                   f"{(kw['n_steps'] or 250) + 1} bandwidths")
     # the workload only (identical in both arms); measured figures sit outside `config`
     S_cfg = (kw["n_steps"] or 250) + 1
     config = {"workload": wl_name, "grid_points": int(np.prod(gspec["dims"])), "bandwidths": S_cfg,
@@ -393,7 +401,7 @@ def main():
     # fixture's) against the FP64 oracle's committed result; recomputed here, outside the
     # timed region (the estimation is deterministic)
     parity = None
-    if not args.no_parity and not args.bandwidth_steps and rank == 0:
+    if not args.no_parity and not small and rank == 0:
         sys.path.insert(0, os.path.join(REPO, "tests", "golden"))
         import config_parity as cp
         z = cp.load(args.workload)
@@ -433,7 +441,7 @@ def main():
                 "wall_ms_per_step": [round(v, 2) for v in e2e_walls] if e2e_value else None},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
-                     "traffic": measured_traffic(args.workload) if not args.bandwidth_steps else None,
+                     "traffic": measured_traffic(args.workload) if not small else None,
                      "algorithmic_bytes": alg_bytes,
                      "kernel": "engine_kernel (persistent step engine: all bandwidth steps, one launch)",
                      "peak_source": peak_kind, "step_ms_per_estimation": step_ms,
@@ -445,7 +453,7 @@ def main():
     }
     if parity is not None:
         line["parity"] = parity
-    if not args.no_batched and args.workload == "c2" and not args.bandwidth_steps:
+    if not args.no_batched and args.workload == "c2" and not small:
         # the metric's "vs plain GPU form" part: the batched mix of 256 estimations, the same
         # set on the plain form (one estimation per call, per-bandwidth-step launches)
         args.steps, args.warmup = args.batched_steps, 1

@@ -239,18 +239,17 @@ __device__ void axis_tiles(double2 *smem, double2 *smem2, const double2 *sm_tw, 
   for (int u = 0; u < ntiles; ++u) {
     double2 v[8];
     load(base, v);
-    if (pf && u + 1 < ntiles) {
-      const int64_t Lw0 = (first_tile + u + 1) * P::NL;
-      const int64_t b0 = (Lw0 / inner) * P::N * inner + (Lw0 % inner);
+    const int64_t nbase = u + 1 < ntiles ? base_of(u + 1) : base;
+    if (pf && u + 1 < ntiles) {  // the tile's first line starts I::line() elements earlier
+      const double2 *b0 = in + nbase - I::line();
       for (int k = threadIdx.x; k < P::N; k += kEngineThreads)
-        prefetch_l2(in + b0 + (int64_t)k * inner, (uint32_t)(P::NL * sizeof(double2)));
+        prefetch_l2(b0 + (int64_t)k * inner, (uint32_t)(P::NL * sizeof(double2)));
     }
     if constexpr (FROM_SPECTRA) {
       const double ncl = line_scale(E, ps, (first_tile + u) * P::NL + I::line());
 #pragma unroll
       for (int r = 0; r < 8; ++r) v[r] = cscale(v[r], f[in_pos<LOGN>(t, r)] * ncl);
     }
-    const int64_t nbase = u + 1 < ntiles ? base_of(u + 1) : base;
     tile_fft_reg<LOGN, 1, true, kEL<LOGN>, true>(smem, v, sm_tw, smem2);
 #pragma unroll
     for (int i = 0; i < 8; ++i) __stcg(out + base + (int64_t)out_pos<LOGN>(t, i) * inner, v[i]);
