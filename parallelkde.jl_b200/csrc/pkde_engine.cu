@@ -219,15 +219,20 @@ __device__ void axis_tiles(double2 *smem, double2 *smem2, const double2 *sm_tw, 
   using P = EP<LOGN>;
   using I = TileIdx<LOGN, true, kEL<LOGN>>;
   const int t = I::bfly();
-  auto base_of = [&](int u) {
-    const int64_t Lw = (first_tile + u) * P::NL + I::line();
-    return (Lw / inner) * P::N * inner + (Lw % inner);
-  };
+  // The thread's line Lw = (first_tile + u) NL + line() starts at (Lw / inner) N inner +
+  // Lw % inner; quotient and remainder advance by NL lines per tile (no division per tile).
+  // Element k of the line is k inner further; its butterfly's elements are t + c (c a
+  // compile-time constant of the position), so every offset is tin + c inner.
+  const int64_t plane = (int64_t)P::N * inner;
+  const int64_t Lw0 = first_tile * P::NL + I::line();
+  int64_t lq = Lw0 / inner, lr = Lw0 % inner;
+  const int64_t tin = (int64_t)t * inner;
   auto load = [&](int64_t base, double2 *x) {
+    const double2 *p = in + base + tin;
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-      const int64_t off = base + (int64_t)in_pos<LOGN>(t, r) * inner;
-      x[r] = FROM_SPECTRA ? __ldcs(in + off) : __ldcg(in + off);
+      const double2 *q = p + (int64_t)(in_pos<LOGN>(t, r) - t) * inner;
+      x[r] = FROM_SPECTRA ? __ldcs(q) : __ldcg(q);
     }
   };
   // The next tile's rows are brought into L2 (bulk prefetch, no registers) while this tile
@@ -235,11 +240,16 @@ __device__ void axis_tiles(double2 *smem, double2 *smem2, const double2 *sm_tw, 
   // is N segments of NL * 16 contiguous bytes.  Holding the next tile in registers instead
   // spilled registers to local memory.
   const bool pf = inner % P::NL == 0;
-  int64_t base = base_of(0);
+  int64_t base = lq * plane + lr;
   for (int u = 0; u < ntiles; ++u) {
     double2 v[8];
     load(base, v);
-    const int64_t nbase = u + 1 < ntiles ? base_of(u + 1) : base;
+    int64_t nbase = base;
+    if (u + 1 < ntiles) {
+      lr += P::NL;
+      while (lr >= inner) lr -= inner, ++lq;
+      nbase = lq * plane + lr;
+    }
     if (pf && u + 1 < ntiles) {  // the tile's first line starts I::line() elements earlier
       const double2 *b0 = in + nbase - I::line();
       for (int k = threadIdx.x; k < P::N; k += kEngineThreads)
@@ -251,8 +261,9 @@ __device__ void axis_tiles(double2 *smem, double2 *smem2, const double2 *sm_tw, 
       for (int r = 0; r < 8; ++r) v[r] = cscale(v[r], f[in_pos<LOGN>(t, r)] * ncl);
     }
     tile_fft_reg<LOGN, 1, true, kEL<LOGN>, true>(smem, v, sm_tw, smem2);
+    double2 *o = out + base + tin;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) __stcg(out + base + (int64_t)out_pos<LOGN>(t, i) * inner, v[i]);
+    for (int i = 0; i < 8; ++i) __stcg(o + (int64_t)(out_pos<LOGN>(t, i) - t) * inner, v[i]);
     base = nbase;
   }
 }
