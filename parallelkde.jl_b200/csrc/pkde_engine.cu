@@ -275,6 +275,13 @@ __device__ __forceinline__ double vmr_of(double Mv, double Vv, double inv_n) {
   const double v = fabs(Vv) * inv_n - m * m;
   return div_nr(v, m);
 }
+// 1/i for the Welford updates over bootstraps i = 1..kRecip-1, each the IEEE quotient
+// (filled once per device from the host's division): the final pass reads it with a
+// CTA-uniform index instead of dividing twice per pair in every thread.
+constexpr int kRecip = 4096;
+__constant__ double c_recip[kRecip];
+__device__ __forceinline__ double recip_of(int i) { return i < kRecip ? c_recip[i] : 1.0 / (double)i; }
+
 __device__ __forceinline__ void welford(double x, double inv, double &mean, double &m2) {
   const double delta = x - mean;
   mean = fma(delta, inv, mean);
@@ -307,7 +314,7 @@ __device__ void vmr_tile(double2 *smem, double2 *state, double2 *sm_tw, const do
     for (int r = 0; r < 8; ++r) w[r] = __ldcg(ws + in_pos<LOGN>(t, r));
     tile_fft_reg<LOGN, 1, false, kEL<LOGN>>(smem, w, sm_tw);
     const int b = b0 + 2 * p;
-    const double inv_a = 1.0 / (double)(b + 1), inv_b = 1.0 / (double)(b + 2);
+    const double inv_a = recip_of(b + 1), inv_b = recip_of(b + 2);
     const bool has_b = b + 1 < nboot;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -421,7 +428,7 @@ __device__ void vmr_tile_gen(double2 *smem, double2 *state, const double2 *in, i
     __syncthreads();
     const double2 *rw = smem_fft<1>(bufA, bufB, pitch, TL, plan, tw);
     const int b = b0 + 2 * p;
-    const double inv_a = 1.0 / (double)(b + 1), inv_b = 1.0 / (double)(b + 2);
+    const double inv_a = recip_of(b + 1), inv_b = recip_of(b + 2);
     const bool has_b = b + 1 < nboot;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -616,7 +623,7 @@ __device__ void vmr_tile_mix(double2 *tile, double2 *state, const double2 *sm_tw
     }
     mix_fft<T>(tile, sm_tw, ro, v);
     const int b = b0 + 2 * p;
-    const double inv_a = 1.0 / (double)(b + 1), inv_b = 1.0 / (double)(b + 2);
+    const double inv_a = recip_of(b + 1), inv_b = recip_of(b + 2);
     const bool has_b = b + 1 < nboot;
 #pragma unroll
     for (int it = 0; it < T::PER; ++it) {
@@ -1130,6 +1137,12 @@ EngineEst describe(const EngineArgs &A) {
 
 void run_engine_batch(pkde_ctx *ctx, const EngineArgs *args, int count, cudaStream_t st) {
   if (count < 1) return;
+  if (!ctx->recip_ready) {
+    std::vector<double> r(kRecip, 0.0);
+    for (int i = 1; i < kRecip; ++i) r[i] = 1.0 / (double)i;
+    PKDE_CUDA_TRY(cudaMemcpyToSymbol(c_recip, r.data(), sizeof(double) * kRecip));
+    ctx->recip_ready = true;
+  }
   std::vector<EngineEst> est(count);
   std::vector<std::array<FftPlan, 4>> plans(count);
   std::vector<std::vector<int64_t>> rs(count);

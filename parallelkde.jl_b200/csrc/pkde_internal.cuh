@@ -116,6 +116,7 @@ struct pkde_ctx {
   // slots of at most 64 MB or one pair)
   bool tune_wide = true;
   bool tune_loaded = false;
+  bool recip_ready = false;  // the step engine's table of 1/i is in this device's constant memory
   std::map<std::string, std::array<int, 3>> tune;
   // polls a step-engine dependency wait makes before it gives up (pkde_set_wait_limit)
   int64_t wait_limit = 20000000;
