@@ -350,30 +350,35 @@ __global__ void quantize_sorted_kernel(GridDev g, const double *__restrict__ rh,
   }
 }
 
-// Scatter in cell order into the paired spectra slots.  Work item d = (b, i), b-major,
-// b = nboot the identity (multiplicity 1).  Warp lanes hold consecutive items: keys
-// (b, cell) are non-decreasing along the warp, so equal keys are contiguous and an
-// inclusive segmented scan sums each run; the run's last lane adds it with one atomic.
+// Scatter in cell order into the paired spectra slots.  Work item d = (chunk c, i),
+// c-major: sample position i (cell order) for the BC resamples b = c BC .. c BC + BC - 1
+// (b = nboot the identity, multiplicity 1).  The thread loads its sample's quantised
+// corner terms once and reuses them for every resample of its chunk (the term arrays,
+// 4 x 2^N x n words, need not stay in L2 across resamples).  Warp lanes hold consecutive
+// items of one chunk, so in every iteration they share b and their keys (b, cell) are
+// non-decreasing along the warp: equal keys are contiguous and an inclusive segmented
+// scan sums each run; the run's last lane adds it with one atomic per part.
 template <int N>
 __global__ void weight_sorted_kernel(const uint32_t *__restrict__ cell_sorted, int64_t n, int64_t nboot, int64_t G,
                                      const int64_t *__restrict__ corner_off, const uint32_t *__restrict__ mult,
                                      const unsigned long long *__restrict__ qm,
                                      const unsigned long long *__restrict__ qv, const long long *__restrict__ qm_lo,
                                      const long long *__restrict__ qv_lo, unsigned long long *__restrict__ out,
-                                     unsigned long long *__restrict__ out_lo, int64_t npairs) {
+                                     unsigned long long *__restrict__ out_lo, int64_t npairs, int BC, int64_t nchunk) {
   constexpr int nc = 1 << N;
+  constexpr bool REG = N <= 3;  // terms held in registers (4-D: re-read, from L1)
   const int lane = threadIdx.x & 31;
-  const int64_t total = (nboot + 1) * n;
+  const int64_t total = nchunk * n;
   // every lane of a warp runs the same number of iterations (the loop bound is rounded
-  // up to whole warps), so the shuffles always see all 32 lanes
+  // up to whole warps, the resample loop has the same trip count in every lane), so the
+  // shuffles always see all 32 lanes
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t d = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; d - lane < total; d += stride) {
     const bool act = d < total;
-    const int64_t b = act ? d / n : 0;
-    const int64_t i = act ? d - b * n : 0;
-    const uint32_t m = act ? (b == nboot ? 1u : mult[b * n + i]) : 0u;
+    const int64_t c = act ? d / n : 0;
+    const int64_t i = act ? d - c * n : 0;
     const uint32_t c0 = act ? cell_sorted[i] : 0u;
-    const unsigned long long key = act ? (((unsigned long long)b << 32) | c0) : ~0ull - (unsigned long long)lane;
+    const unsigned long long key = act ? (((unsigned long long)c << 32) | c0) : ~0ull - (unsigned long long)lane;
     bool same[5];
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
@@ -381,39 +386,59 @@ __global__ void weight_sorted_kernel(const uint32_t *__restrict__ cell_sorted, i
       same[k] = lane >= (1 << k) && up == key;
     }
     const bool last = __shfl_down_sync(0xffffffffu, key, 1) != key || lane == 31;
-    const int64_t p = b >> 1, half = b & 1;
+    unsigned long long rqm[REG ? nc : 1], rqv[REG ? nc : 1];
+    long long rlm[REG ? nc : 1], rlv[REG ? nc : 1];
+    if constexpr (REG) {
 #pragma unroll
-    for (int c = 0; c < nc; ++c) {
-      const int64_t cc = (int64_t)c0 + (act ? corner_off[c] : 0);
-      unsigned long long vm = m ? (unsigned long long)m * qm[c * n + i] : 0ull;
-      unsigned long long vv = (m && b < nboot) ? (unsigned long long)m * qv[c * n + i] : 0ull;
-      // low parts: signed, summed modulo 2^64 (the true sums fit in 63 bits)
-      unsigned long long lm = m ? (unsigned long long)((long long)m * qm_lo[c * n + i]) : 0ull;
-      unsigned long long lv = (m && b < nboot) ? (unsigned long long)((long long)m * qv_lo[c * n + i]) : 0ull;
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        const unsigned long long um = __shfl_up_sync(0xffffffffu, vm, 1 << k);
-        const unsigned long long uv = __shfl_up_sync(0xffffffffu, vv, 1 << k);
-        const unsigned long long ulm = __shfl_up_sync(0xffffffffu, lm, 1 << k);
-        const unsigned long long ulv = __shfl_up_sync(0xffffffffu, lv, 1 << k);
-        if (same[k]) {
-          vm += um;
-          vv += uv;
-          lm += ulm;
-          lv += ulv;
-        }
+      for (int q = 0; q < nc; ++q) {
+        rqm[q] = act ? qm[q * n + i] : 0ull;
+        rqv[q] = act ? qv[q * n + i] : 0ull;
+        rlm[q] = act ? qm_lo[q * n + i] : 0ll;
+        rlv[q] = act ? qv_lo[q * n + i] : 0ll;
       }
-      if (act && last) {
-        if (b == nboot) {
-          const int64_t o = (2 * npairs * G + cc) * 2;
-          if (vm) atomicAdd(&out[o], vm);
-          if (lm) atomicAdd(&out_lo[o], lm);
-        } else {
-          const int64_t om = ((2 * p) * G + cc) * 2 + half, ov = ((2 * p + 1) * G + cc) * 2 + half;
-          if (vm) atomicAdd(&out[om], vm);
-          if (vv) atomicAdd(&out[ov], vv);
-          if (lm) atomicAdd(&out_lo[om], lm);
-          if (lv) atomicAdd(&out_lo[ov], lv);
+    }
+    for (int bb = 0; bb < BC; ++bb) {
+      const int64_t b = c * BC + bb;
+      const bool ab = act && b <= nboot;
+      const uint32_t m = ab ? (b == nboot ? 1u : mult[b * n + i]) : 0u;
+      const int64_t p = b >> 1, half = b & 1;
+#pragma unroll
+      for (int q = 0; q < nc; ++q) {
+        const int64_t cc = (int64_t)c0 + (act ? corner_off[q] : 0);
+        const unsigned long long tm = REG ? rqm[q] : (m ? __ldg(qm + q * n + i) : 0ull);
+        const unsigned long long tv = REG ? rqv[q] : (m ? __ldg(qv + q * n + i) : 0ull);
+        const long long tlm = REG ? rlm[q] : (m ? __ldg(qm_lo + q * n + i) : 0ll);
+        const long long tlv = REG ? rlv[q] : (m ? __ldg(qv_lo + q * n + i) : 0ll);
+        unsigned long long vm = m ? (unsigned long long)m * tm : 0ull;
+        unsigned long long vv = (m && b < nboot) ? (unsigned long long)m * tv : 0ull;
+        // low parts: signed, summed modulo 2^64 (the true sums fit in 63 bits)
+        unsigned long long lm = m ? (unsigned long long)((long long)m * tlm) : 0ull;
+        unsigned long long lv = (m && b < nboot) ? (unsigned long long)((long long)m * tlv) : 0ull;
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          const unsigned long long um = __shfl_up_sync(0xffffffffu, vm, 1 << k);
+          const unsigned long long uv = __shfl_up_sync(0xffffffffu, vv, 1 << k);
+          const unsigned long long ulm = __shfl_up_sync(0xffffffffu, lm, 1 << k);
+          const unsigned long long ulv = __shfl_up_sync(0xffffffffu, lv, 1 << k);
+          if (same[k]) {
+            vm += um;
+            vv += uv;
+            lm += ulm;
+            lv += ulv;
+          }
+        }
+        if (ab && last) {
+          if (b == nboot) {
+            const int64_t o = (2 * npairs * G + cc) * 2;
+            if (vm) atomicAdd(&out[o], vm);
+            if (lm) atomicAdd(&out_lo[o], lm);
+          } else {
+            const int64_t om = ((2 * p) * G + cc) * 2 + half, ov = ((2 * p + 1) * G + cc) * 2 + half;
+            if (vm) atomicAdd(&out[om], vm);
+            if (vv) atomicAdd(&out[ov], vv);
+            if (lm) atomicAdd(&out_lo[om], lm);
+            if (lv) atomicAdd(&out_lo[ov], lv);
+          }
         }
       }
     }
@@ -789,10 +814,13 @@ void dirac_job_phase_b(pkde_ctx *ctx, DiracJob &j, const int *hmisc, cudaStream_
   PKDE_CUDA_TRY(cudaMemsetAsync(j.acc_lo, 0, sizeof(double2) * (2 * npairs + 1) * G, st));
   {
     ::pkde::Trace _tr(ctx, PKDE_PHASE_BINNING, st);
-    const int blocks = grid_blocks(ctx, nslots * n);
+    // resamples in chunks of at most 16, as even as possible (65 = 5 x 13, 33 = 3 x 11)
+    const int64_t nchunk = (nslots + 15) / 16;
+    const int BC = (int)((nslots + nchunk - 1) / nchunk);
+    const int blocks = grid_blocks(ctx, nchunk * n);
 #define PKDE_WS(NN)                                                                                          \
   weight_sorted_kernel<NN><<<blocks, kThreads, 0, st>>>(j.cell_sorted, n, nboot, G, corner_off, j.mult, qm, qv,   \
-                                                        j.qm_lo, j.qv_lo, acc, j.acc_lo, npairs)
+                                                        j.qm_lo, j.qv_lo, acc, j.acc_lo, npairs, BC, nchunk)
     switch (N) {
       case 1: PKDE_WS(1); break;
       case 2: PKDE_WS(2); break;

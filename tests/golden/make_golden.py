@@ -157,7 +157,7 @@ def add_stability(name, variants, workers):
 
 
 def add_sampled_stability(name, trace_variants, samples, heldout, workers, seed=1, batch=16, cache=None,
-                          target=5e-4):
+                          target=2.5e-4):
     """Extend the fixture's rounding-unstable set with sampled rounding realisations.
 
     A union over a handful of FP64 implementations under-covers the points whose decision
@@ -170,13 +170,15 @@ def add_sampled_stability(name, trace_variants, samples, heldout, workers, seed=
     give k rounding differences D_i = F_i - F0, each with the step-to-step correlation of
     real rounding.  Each sample replays the selection on F0 + sum_i c_i D_i, c ~ N(0, 1/k)
     (the variance of one more independent implementation's difference from the
-    reference), so a point's flip frequency q over the samples estimates the probability
+    reference), so a point's flip frequency over the samples estimates the probability q
     that an independent FP64 implementation selects another step there.  The unstable set
-    is the variants' own flips plus the points of highest q, as few as leave an expected
-    flip rate sum(q) / |stable| <= `target` (half the 0.1 % that parity allows) on the
-    remaining, stable points, and at most 0.1 expected flips there on small grids (one
-    flip near the mode of a 1-D density of 1,024 points already moves it by 2e-4
-    relative L2).  `rounding_rate` (the mean of q over the grid: the expected
+    is the variants' own flips plus the points ranked highest by the frequency in one half
+    of the samples, as few as leave an expected flip rate <= `target` (a quarter of the
+    0.1 % that parity allows) on the remaining, stable points, that rate estimated from
+    the other half: ranked and scored by the same counts, the points kept as stable are
+    the ones whose count came out low, and their residual is underestimated (by 3x on
+    C2).  On small grids at most 0.1 expected flips are left (one flip near the mode of a
+    1-D density of 1,024 points already moves it by 2e-4 relative L2).  `rounding_rate` (the mean of q over the grid: the expected
     flip rate of an independent implementation) is recorded beside the whole-grid flip
     rates of the `heldout` implementations (real ones, run afterwards and not used to
     build the set) as a calibration check, with their agreement on the stable points.
@@ -223,22 +225,24 @@ def add_sampled_stability(name, trace_variants, samples, heldout, workers, seed=
     t0 = og.initial_bandwidth(grid)
     rng = np.random.default_rng(seed)
     k = len(trace_variants)
-    flips = np.zeros(G, dtype=np.int32)
+    flips = np.zeros((2, G), dtype=np.int32)  # the two halves of the samples
     done = 0
     while done < samples:
         m = min(batch, samples - done)
         C = (rng.standard_normal((m, k)) / math.sqrt(k)).astype(np.float32)
         steps = (np.asarray(F0[s])[None, :] + (C @ D[:, s, :]).astype(np.float64) for s in range(S))
         sel = og.select_from_trace(steps, times, t0, steps_low, steps_over, eps)
-        flips += np.sum(sel != ref_sel[None, :], axis=0).astype(np.int32)
+        flips[0 if done < samples // 2 else 1] += np.sum(sel != ref_sel[None, :], axis=0).astype(np.int32)
         done += m
         print(f"config_{name}: {done} samples, mean flip rate {flips.sum() / (done * G):.5f} "
               f"({time.time() - t_start:.0f} s)", flush=True)
-    q = flips / float(samples)
-    # the fewest points of highest q that leave sum(q) / |stable| <= target on the rest
-    order = np.argsort(-q, kind="stable")
-    qs = q[order]
-    rest = np.cumsum(qs[::-1])[::-1]  # rest[j]: sum of q over order[j:]
+    half = (samples // 2 + batch - 1) // batch * batch  # the first half: whole batches
+    qa = flips[0] / float(half)
+    qb = flips[1] / float(samples - half)
+    q = flips.sum(0) / float(samples)
+    # the fewest points of highest qa that leave sum(qb) / |stable| <= target on the rest
+    order = np.argsort(-qa, kind="stable")
+    rest = np.cumsum(qb[order][::-1])[::-1]  # rest[j]: sum of qb over order[j:]
     nstable = G - np.arange(G)
     ok = np.nonzero(rest <= np.minimum(target * nstable, np.maximum(0.1, 1e-4 * nstable)))[0]
     cut = int(ok[0]) if ok.size else G
@@ -246,9 +250,8 @@ def add_sampled_stability(name, trace_variants, samples, heldout, workers, seed=
     sampled[order[:cut]] = True
     unstable = sampled | real
     stable = ~unstable
-    print(f"config_{name}: sampled set {np.mean(sampled):.5f} (q >= {qs[cut - 1] if cut else 1:.4f}), union "
-          f"{np.mean(unstable):.5f}, expected flip rate on the stable points {q[stable].sum() / max(stable.sum(), 1):.6f}, "
-          f"over the grid {q.mean():.5f}", flush=True)
+    print(f"config_{name}: sampled set {np.mean(sampled):.5f}, union {np.mean(unstable):.5f}, expected flip rate "
+          f"on the stable points {qb[stable].sum() / max(stable.sum(), 1):.6f}, over the grid {q.mean():.5f}", flush=True)
     hagree = []
     for v in heldout:
         if cpath and os.path.exists(cpath(f"sel_{v}")):
@@ -269,7 +272,7 @@ def add_sampled_stability(name, trace_variants, samples, heldout, workers, seed=
     z["rounding_seed"] = np.int64(seed)
     z["rounding_target"] = np.float64(target)
     z["rounding_rate"] = np.float64(q.mean())
-    z["rounding_rate_stable"] = np.float64(q[stable].sum() / max(stable.sum(), 1))
+    z["rounding_rate_stable"] = np.float64(qb[stable].sum() / max(stable.sum(), 1))
     z["heldout"] = np.array(list(heldout))
     z["heldout_agree"] = np.array(hagree).reshape(-1, 2)
     np.savez_compressed(path, **z)

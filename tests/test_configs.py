@@ -75,13 +75,14 @@ def test_oracle_reproduces_c1(oracle):
     assert np.max(np.abs(res.density - z["density"])) <= 1e-13 * np.max(z["density"])
 
 
-def _heldout_bar(z):
-    """Agreement a held-out implementation must reach on the stable points: 99.9 %, or all
-    but one point where 0.1 % of them is less than one point (C1: ~1,000 stable points,
-    where the set's expected 0.1 flips per implementation make one flip in one of five
-    implementations an even bet)."""
+def _heldout_ok(z, agree_stable):
+    """Whether a held-out implementation's agreement on the stable points meets the bar:
+    at most 0.1 % of them flipped, or one point where 0.1 % of them is less than one point
+    (C1: ~1,000 stable points, where the set's expected 0.1 flips per implementation make
+    one flip in one of five implementations an even bet)."""
     n = int(np.sum(~np.unpackbits(z["unstable"], count=int(np.prod(z["dims"]))).astype(bool)))
-    return min(AGREE, 1.0 - 1.0 / n)
+    flips = int(round((1.0 - agree_stable) * n))
+    return flips <= max(1, int((1.0 - AGREE) * n))
 
 
 @pytest.mark.parametrize("name", CONFIGS)
@@ -96,11 +97,10 @@ def test_stable_set_complete(name):
         pytest.skip("fixture without held-out implementations")
     assert len(z["heldout"]) >= 2
     assert float(z["rounding_rate_stable"]) <= 5e-4
-    bar = _heldout_bar(z)
     for v, (whole, stable) in zip(z["heldout"], z["heldout_agree"]):
         print(f"{name}: held-out {v}: flip rate {1 - whole:.5f} on the grid (sampled realisations "
               f"{float(z['rounding_rate']):.5f}), agreement {stable:.5f} on the stable points")
-        assert stable >= bar
+        assert _heldout_ok(z, stable)
         assert 1 - whole <= 3 * float(z["rounding_rate"]) + 1e-3
 
 
@@ -118,7 +118,7 @@ def test_stable_set_heldout_live_c1(oracle):
     p = parity(res.density, res.selected_step, z)
     rec = z["heldout_agree"][list(z["heldout"]).index("mkl")]
     assert p["agree"] == pytest.approx(rec[0]) and p["agree_stable"] == pytest.approx(rec[1])
-    assert p["agree_stable"] >= _heldout_bar(z)
+    assert _heldout_ok(z, p["agree_stable"])
 
 
 @pytest.mark.gpu
