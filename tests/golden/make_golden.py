@@ -157,7 +157,7 @@ def add_stability(name, variants, workers):
 
 
 def add_sampled_stability(name, trace_variants, samples, heldout, workers, seed=1, batch=16, cache=None,
-                          target=2.5e-4):
+                          target=1e-4):
     """Extend the fixture's rounding-unstable set with sampled rounding realisations.
 
     A union over a handful of FP64 implementations under-covers the points whose decision
@@ -173,12 +173,12 @@ def add_sampled_stability(name, trace_variants, samples, heldout, workers, seed=
     reference), so a point's flip frequency over the samples estimates the probability q
     that an independent FP64 implementation selects another step there.  The unstable set
     is the variants' own flips plus the points ranked highest by the frequency in one half
-    of the samples, as few as leave an expected flip rate <= `target` (a quarter of the
-    0.1 % that parity allows) on the remaining, stable points, that rate estimated from
-    the other half: ranked and scored by the same counts, the points kept as stable are
-    the ones whose count came out low, and their residual is underestimated (by 3x on
-    C2).  On small grids at most 0.1 expected flips are left (one flip near the mode of a
-    1-D density of 1,024 points already moves it by 2e-4 relative L2).  `rounding_rate` (the mean of q over the grid: the expected
+    of the samples, as few as leave an expected flip rate <= `target` (a tenth of the
+    0.1 % that parity allows; on C1's ~1,000 points 0.1 expected flips, where one flip near
+    the mode already moves the density by 2e-4 relative L2) on the remaining, stable
+    points, that rate estimated from the other half: ranked and scored by the same counts,
+    the points kept as stable are the ones whose count came out low, and their residual
+    is underestimated (by 3x on C2).  `rounding_rate` (the mean of q over the grid: the expected
     flip rate of an independent implementation) is recorded beside the whole-grid flip
     rates of the `heldout` implementations (real ones, run afterwards and not used to
     build the set) as a calibration check, with their agreement on the stable points.
@@ -244,7 +244,7 @@ def add_sampled_stability(name, trace_variants, samples, heldout, workers, seed=
     order = np.argsort(-qa, kind="stable")
     rest = np.cumsum(qb[order][::-1])[::-1]  # rest[j]: sum of qb over order[j:]
     nstable = G - np.arange(G)
-    ok = np.nonzero(rest <= np.minimum(target * nstable, np.maximum(0.1, 1e-4 * nstable)))[0]
+    ok = np.nonzero(rest <= target * nstable)[0]
     cut = int(ok[0]) if ok.size else G
     sampled = np.zeros(G, dtype=bool)
     sampled[order[:cut]] = True
