@@ -66,16 +66,57 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled every 100 ms during the timed region: NVML
+    in a thread of this process (only the clock and the reason mask are read), else an
+    `nvidia-smi` sampler.  (Measured on the 2-D workload: with `nvidia-smi -lms 100`
+    running, the device waited for the host's launches and synchronisations ~8 ms per
+    estimation -- p50 65.9 ms against 57.5 ms -- the NVML thread costs nothing visible.)"""
+
+    NAMES = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
     def __init__(self, index):
-        import tempfile
         self.index = index
         self.proc = None
-        fd, self.path = tempfile.mkstemp(prefix="pkde_clocks_", suffix=".csv")
-        os.close(fd)
+        self.thread = None
+        self.samples = []
+        self.path = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:  # the CUDA device's own GPU, whatever CUDA_VISIBLE_DEVICES maps
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.stop_flag = threading.Event()
+
+            def run():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(reasons(h))))
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(0.1)
+
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
+        import tempfile
+        fd, self.path = tempfile.mkstemp(prefix="pkde_clocks_", suffix=".csv")
+        os.close(fd)
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
@@ -86,6 +127,15 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            time.sleep(0.15)
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            if not self.samples:
+                return None
+            reasons = sorted(nm for nm, bit in self.NAMES.items() if any(r & bit for _, r in self.samples))
+            return {"sm_mhz": statistics.median(c for c, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(self.samples), "sampler": "nvml"}
         if self.proc is None:
             return None
         time.sleep(0.25)
@@ -114,7 +164,8 @@ class Clocks:
             pass
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "sampler": "nvidia-smi"}
 
 
 def dist_setup(args):
