@@ -568,6 +568,10 @@ __device__ void axis_tiles_mix(double2 *tile, const double2 *sm_tw, const double
   using T = MixTile<R, LM, X::NLA, 1>;
   const MixRole<T> ro;
   const int lc = threadIdx.x % X::NLA;  // the combine line (NLA divides the block)
+  // With `inner` a multiple of NLA a tile's lines are adjacent in memory: N segments of
+  // NLA * 16 contiguous bytes, which are brought into L2 for the next tile while this one
+  // is transformed (as in the power-of-two column passes).
+  const bool pf = inner % X::NLA == 0;
   for (int u = 0; u < ntiles; ++u) {
     const int64_t L0 = (first_tile + u) * X::NLA;
     const int64_t Lf = L0 + ro.l, Lc = L0 + lc;
@@ -582,6 +586,12 @@ __device__ void axis_tiles_mix(double2 *tile, const double2 *sm_tw, const double
       const int64_t off = bf + (int64_t)pos * inner;
       if constexpr (FROM_SPECTRA) v[r] = ro.act ? cscale(__ldcs(in + off), f[pos] * cl) : make_double2(0.0, 0.0);
       else v[r] = ro.act ? __ldcg(in + off) : make_double2(0.0, 0.0);
+    }
+    if (pf && u + 1 < ntiles) {
+      const int64_t Ln = L0 + X::NLA;  // first line of the next tile (Ln % inner + NLA <= inner)
+      const double2 *b0 = in + (Ln / inner) * X::N * inner + (Ln % inner);
+      for (int k = threadIdx.x; k < X::N; k += kEngineThreads)
+        prefetch_l2(b0 + (int64_t)k * inner, (uint32_t)(X::NLA * sizeof(double2)));
     }
     mix_fft<T>(tile, sm_tw, ro, v);
 #pragma unroll
