@@ -1,6 +1,7 @@
 """Benchmark of the :gradepro estimator on B200 (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2|c1|c3]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+        [--workload c2|c1|c3|shape --dims 96x96x96|batched|batched-small|served]
 
 A "step" is one complete :gradepro estimation (binning, forward transforms, every
 bandwidth step, convergence, outputs) of one sample set.  The default workload is the
@@ -33,8 +34,12 @@ UNIT = "grid-pt·steps/s"
 HBM_FALLBACK_GBS = 6650.0
 
 
-def workload(name):
+def workload(name, dims=None, samples=200_000):
     from pkde_b200 import workloads as W
+    if name == "shape":  # one estimation of a batched-mix shape class (profiling single shapes)
+        d = tuple(int(v) for v in dims.lower().split("x"))
+        x = W.random_mixture(len(d), samples, np.random.default_rng(5))
+        return x, dict(dims=d), dict(n_bootstraps=32, n_steps=100)
     if name == "c1":
         x, spec = W.gaussian_1d()
         return x, dict(dims=spec["dims"], grid_padding=spec["grid_padding"]), dict(n_bootstraps=100, n_steps=None)
@@ -315,7 +320,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "batched", "batched-small", "served"])
+    ap.add_argument("--workload", default="c2",
+                    choices=["c1", "c2", "c3", "shape", "batched", "batched-small", "served"])
+    ap.add_argument("--dims", default="96x96x96",
+                    help="--workload shape: grid dims of one estimation like the batched mix's (B=32, 101 "
+                         "bandwidths, a random 1-4 component Gaussian mixture of --samples samples)")
+    ap.add_argument("--samples", type=int, default=200_000, help="--workload shape: samples")
     ap.add_argument("--rate", type=float, default=50.0, help="requests/s (--workload served)")
     ap.add_argument("--requests", type=int, default=64, help="requests (--workload served)")
     ap.add_argument("--lanes", type=int, default=2, help="serving lanes (--workload served)")
@@ -347,7 +357,7 @@ def main():
         return run_batched(args, world, rank, local, dist)
     if args.workload == "served":
         return run_served(args, world, rank, local, dist)
-    x, gspec, kw = workload(args.workload)
+    x, gspec, kw = workload(args.workload, args.dims, args.samples)
     if args.bandwidth_steps:
         kw["n_steps"] = args.bandwidth_steps
     if args.bootstraps:
@@ -355,7 +365,9 @@ def main():
     small = bool(args.bandwidth_steps or args.bootstraps)  # a profiling case, not the workload
     wl_name = {"c1": "1-D N(0,1) n=1e4, 1024 pts, B=100, 251 bandwidths",
                "c2": "2-D 3-GMM n=1e6, 512x512, B=64, 201 bandwidths",
-               "c3": "3-D banana+t3 n=4e6, 128^3, B=32, 151 bandwidths"}[args.workload]
+               "c3": "3-D banana+t3 n=4e6, 128^3, B=32, 151 bandwidths",
+               "shape": (f"{len(gspec['dims'])}-D random Gaussian mixture n={x.shape[1]}, "
+                         f"{'x'.join(map(str, gspec['dims']))}, B=32, 101 bandwidths")}[args.workload]
     if small:
         wl_name = (f"profiling case of {args.workload} ({wl_name.split(',')[0]}): B={kw['n_bootstraps']}, "
                    f"{(kw['n_steps'] or 250) + 1} bandwidths")

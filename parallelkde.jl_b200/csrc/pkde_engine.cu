@@ -618,10 +618,19 @@ __device__ void vmr_tile_mix(double2 *tile, double2 *state, const double2 *sm_tw
   const MixRole<T> ro;
   const int npts = X::NLF * X::N;
   const int64_t rbase = tile_idx * npts;
-  const int lrow = (threadIdx.x % X::NLF) * X::N;
+  // The Welford state sits in shared memory in combine-item order: entry q ITEMS + idx is
+  // point (row idx % NLF, position idx / NLF + M q) of the tile, so consecutive threads
+  // update consecutive entries.  (In point order their rows lie N apart, and N = R M with
+  // M >= 8 is a multiple of 8 16-byte units: every access an 8-way bank conflict.)
+  auto point_of = [](int si) {
+    const int q = si / T::ITEMS, idx = si - q * T::ITEMS;
+    return (idx % X::NLF) * X::N + idx / X::NLF + X::M * q;
+  };
   prefetch_pair(in, G, 0, npairs, rbase, npts);
-  for (int e = threadIdx.x; e < npts; e += blockDim.x)
-    state[e] = first ? make_double2(0.0, 0.0) : make_double2(__ldcg(wst + rbase + e), __ldcg(wst + G + rbase + e));
+  for (int si = threadIdx.x; si < npts; si += blockDim.x) {
+    const int e = point_of(si);
+    state[si] = first ? make_double2(0.0, 0.0) : make_double2(__ldcg(wst + rbase + e), __ldcg(wst + G + rbase + e));
+  }
   for (int p = 0; p < npairs; ++p) {
     prefetch_pair(in, G, p + 1, npairs, rbase, npts);
     const double2 *src = in + (int64_t)(2 * p + ro.a) * G + rbase + ro.l * X::N;
@@ -641,20 +650,21 @@ __device__ void vmr_tile_mix(double2 *tile, double2 *state, const double2 *sm_tw
       double2 z[R], w[R];
       if (mix_combine<T>(tile, twc, it, 0, k2, z)) {
         mix_combine<T>(tile, twc, it, 1, k2, w);
+        const int idx = threadIdx.x + it * kEngineThreads;  // the combine item (k2 = idx / NLF)
 #pragma unroll
         for (int q = 0; q < R; ++q) {
-          const int e = lrow + k2 + X::M * q;
-          double2 st = state[e];
+          double2 st = state[q * T::ITEMS + idx];
           welford(vmr_of(z[q].x, w[q].x, inv_n), inv_a, st.x, st.y);
           if (has_b) welford(vmr_of(z[q].y, w[q].y, inv_n), inv_b, st.x, st.y);
-          state[e] = st;
+          state[q * T::ITEMS + idx] = st;
         }
       }
     }
     __syncthreads();
   }
-  for (int e = threadIdx.x; e < npts; e += blockDim.x) {
-    const double2 st = state[e];
+  for (int si = threadIdx.x; si < npts; si += blockDim.x) {
+    const int e = point_of(si);
+    const double2 st = state[si];
     __stcg(wst + rbase + e, st.x);
     __stcg(wst + G + rbase + e, st.y);
   }
