@@ -921,26 +921,33 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
   {
     std::vector<EngineArgs> lean, wide;
     for (const EngineArgs &A : eng) (engine_register_only(A.grid) ? lean : wide).push_back(A);
-    // Schedules are tuned per shape, one estimation at a time; a launch of many estimations
-    // whose tuned ring slots are wide could need more memory than is free, so then every
-    // slot of that launch is narrowed (the schedule changes time, never results).
-    auto fit = [&](std::vector<EngineArgs> &v) {
-      size_t need = 0;
-      for (const EngineArgs &A : v) need += engine_ring_bytes(A);
+    // Schedules are tuned per shape, one estimation at a time, and the tuned ring slots of
+    // many estimations together can exceed the free memory.  The estimations are then
+    // packed, in call order, into consecutive launches whose rings fit half of it, each
+    // keeping its tuned schedule; only an estimation whose ring alone exceeds that runs
+    // with narrow slots (the schedule changes time, never results).  Narrowing every slot
+    // of a single launch instead cost the batched mix of 256 estimations more than the
+    // launch boundaries do (it ran slower than the same estimations one call each).
+    auto launch_fitting = [&](std::vector<EngineArgs> &v) {
+      if (v.empty()) return;
       size_t freeb = 0, totalb = 0;
       PKDE_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
-      if (need <= (freeb + ctx->buf[BUF_ENGINE].bytes) / 2) return;
-      for (EngineArgs &A : v)
-        if (A.tune_slot_mb > kNarrowSlotMB) A.tune_slot_mb = kNarrowSlotMB;
+      const size_t budget = (freeb + ctx->buf[BUF_ENGINE].bytes) / 2;
+      size_t i = 0;
+      while (i < v.size()) {
+        size_t need = 0, j = i;
+        for (; j < v.size(); ++j) {
+          if (engine_ring_bytes(v[j]) > budget && v[j].tune_slot_mb > kNarrowSlotMB) v[j].tune_slot_mb = kNarrowSlotMB;
+          const size_t r = engine_ring_bytes(v[j]);
+          if (j > i && need + r > budget) break;
+          need += r;
+        }
+        run_engine_batch(ctx, v.data() + i, (int)(j - i), st);
+        i = j;
+      }
     };
-    if (!lean.empty()) {
-      fit(lean);
-      run_engine_batch(ctx, lean.data(), (int)lean.size(), st);
-    }
-    if (!wide.empty()) {
-      fit(wide);
-      run_engine_batch(ctx, wide.data(), (int)wide.size(), st);
-    }
+    launch_fitting(lean);
+    launch_fitting(wide);
   }
   // ---- replace_nans! and outputs
   for (int e = 0; e < count; ++e) {
