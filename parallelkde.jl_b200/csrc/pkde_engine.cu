@@ -560,8 +560,12 @@ __device__ __forceinline__ bool mix_combine(const double2 *tile, const double2 *
   return true;
 }
 
+// The three mixed-radix tile bodies are separate (not inlined) functions: inlined into the
+// persistent kernel beside every other (R, M) instantiation they shared its 128 registers
+// with the item loop's live values and spilled (1.4 KB of stack); compiled on their own
+// they spill nothing (96^3 1.22 -> 1.09 ns per grid-point step, 80^3 1.50 -> 1.14).
 template <int R, int LM, bool FROM_SPECTRA>
-__device__ void axis_tiles_mix(double2 *tile, const double2 *sm_tw, const double2 *twc, const double2 *in,
+__device__ __noinline__ void axis_tiles_mix(double2 *tile, const double2 *sm_tw, const double2 *twc, const double2 *in,
                                double2 *out, int64_t inner, int64_t first_tile, int ntiles, const double *f,
                                const EngineEst &E, const PassScale ps) {
   using X = Mix<R, LM>;
@@ -610,7 +614,7 @@ __device__ void axis_tiles_mix(double2 *tile, const double2 *sm_tw, const double
 // Final pass: NLF rows; the tile holds the z and the w sub-lines of those rows, so each
 // combine item has both transforms of its points for the VMR and the Welford update.
 template <int R, int LM>
-__device__ void vmr_tile_mix(double2 *tile, double2 *state, const double2 *sm_tw, const double2 *twc,
+__device__ __noinline__ void vmr_tile_mix(double2 *tile, double2 *state, const double2 *sm_tw, const double2 *twc,
                              const double2 *in, int npairs, int b0, int nboot, double inv_n, int64_t G, double *wst,
                              int first, int64_t tile_idx) {
   using X = Mix<R, LM>;
@@ -672,7 +676,7 @@ __device__ void vmr_tile_mix(double2 *tile, double2 *state, const double2 *sm_tw
 
 // Means pass over the same NLF rows (one array; the second array's threads idle).
 template <int R, int LM>
-__device__ void means_tile_mix(double2 *tile, const double2 *sm_tw, const double2 *twc, const double2 *in,
+__device__ __noinline__ void means_tile_mix(double2 *tile, const double2 *sm_tw, const double2 *twc, const double2 *in,
                                const double *wst, int64_t G, int nboot, double vscale, double dlogt, double eps,
                                int64_t steps_low, int64_t steps_over, const StepState &cs, int step,
                                int64_t tile_idx) {
