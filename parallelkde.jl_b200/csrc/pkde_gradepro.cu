@@ -15,6 +15,7 @@
 //   state    : f_prev1, f_prev2, minima (FP64), counters_low/over (u16), flags (u8),
 //              density (FP64), selected step (i32), final-step means (FP64).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 
@@ -932,7 +933,10 @@ void run_many(pkde_ctx *ctx, const Estimation *ests, int count, cudaStream_t st)
       if (v.empty()) return;
       size_t freeb = 0, totalb = 0;
       PKDE_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
-      const size_t budget = (freeb + ctx->buf[BUF_ENGINE].bytes) / 2;
+      size_t budget = (freeb + ctx->buf[BUF_ENGINE].bytes) / 2;
+      // PKDE_RING_BUDGET_MB caps the budget (tests use it to force one launch per estimation)
+      if (const char *cap = getenv("PKDE_RING_BUDGET_MB"); cap && *cap)
+        budget = std::min(budget, (size_t)std::max(0LL, atoll(cap)) << 20);
       size_t i = 0;
       while (i < v.size()) {
         size_t need = 0, j = i;

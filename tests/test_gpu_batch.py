@@ -249,3 +249,33 @@ def test_wide_ring_slots_keep_results(pk, monkeypatch):
         lib.pkde_destroy(ctx)
     for d, s in outs[1:]:
         assert np.array_equal(d, outs[0][0]) and np.array_equal(s, outs[0][1])
+
+
+def test_batch_packed_into_several_launches(pk, monkeypatch):
+    """When the estimations' tuned ring slots together exceed the memory budget, a batch call
+    packs them into consecutive engine launches that fit (PKDE_RING_BUDGET_MB caps the
+    budget: with 1 MB every estimation gets a launch of its own).  The results equal each
+    estimation's alone result, bit for bit.  N-D estimations only: the 1-D step path's
+    launches count in the same phase."""
+    from pkde_b200 import _lib, raw
+    mix = [m for m in _mix(pk) if len(m[0].dims) >= 2]
+    alone = [_alone(pk, grid, x, kw, seed=100 + e) for e, (grid, x, kw) in enumerate(mix)]  # also tunes
+
+    def engine_launches(jobs):
+        _lib.get_stats(0, reset=True)
+        _lib.set_profiling(_lib.PKDE_PROFILE_STEPS, 0)
+        try:
+            raw.gradepro_batch(jobs)
+        finally:
+            _lib.set_profiling(_lib.PKDE_PROFILE_OFF, 0)
+        return _lib.get_stats(0, reset=True)["phase_launches"]["step_vmr"]
+
+    jobs = _batch_jobs(mix)
+    assert engine_launches(jobs) <= 2  # the lean and the mixed-radix instantiation
+    monkeypatch.setenv("PKDE_RING_BUDGET_MB", "1")
+    packed = _batch_jobs(mix)
+    assert engine_launches(packed) == len(mix)
+    for e, (d, s) in enumerate(alone):
+        assert np.array_equal(packed[e]["density"], d, equal_nan=True), f"estimation {e}"
+        assert np.array_equal(packed[e]["selected"], s), f"estimation {e}"
+        assert np.array_equal(jobs[e]["density"], d, equal_nan=True), f"estimation {e}"
